@@ -1,0 +1,181 @@
+/*
+ * qsim.h -- C-ABI of libqsim.so, the sm_100a gate-application library behind
+ * quict_b200's StateVectorSimulator / DensityMatrixSimulator.
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ *  - A state vector is a contiguous device array of 2^n complex numbers,
+ *    interleaved (re, im), in complex64 (QS_C64) or complex128 (QS_C128).
+ *  - "bit" always means a VECTOR bit: amplitude index i has bit b set iff
+ *    (i >> b) & 1.  A QuICT qubit q of an n-qubit circuit is vector bit n-1-q
+ *    (QuICT/core/qubit/qubit.py:192-213, statevector_simulator.py:170-172).
+ *  - A k-qubit matrix is row-major 2^k x 2^k; matrix-index bit (k-1-j)
+ *    belongs to the j-th listed vector bit ("big-endian over the argument
+ *    list", QuICT/core/utils/utils.py:8-56).
+ *  - Host matrices are passed as complex128 (double re, im pairs) and are
+ *    rounded to the state's precision inside the call, the same rounding as
+ *    numpy's astype(complex64) that QuICT applies (gate.py:945-951).
+ *  - The caller owns every buffer.  The library never allocates device
+ *    memory; scratch comes from a caller workspace whose size the matching
+ *    *_ws_bytes() query returns.
+ *  - Every call is stream-ordered on `stream` (a cudaStream_t; NULL = legacy
+ *    default stream), performs no implicit device synchronisation and returns
+ *    QS_OK or a negative QS_E* code.  qs_last_error() returns a thread-local
+ *    description of the last failure.  No C++ exception crosses the ABI.
+ *
+ * The reference (taofei95/quict) dispatches one CuPy RawKernel per gate from
+ * Python through LinAlgLoader (QuICT/ops/utils/algorithm_loader.py:17-54);
+ * each entry point below names the reference interface it replaces.
+ */
+#ifndef QSIM_H
+#define QSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define QS_OK          0
+#define QS_EINVAL     -1   /* bad argument (qubit out of range, bad kind ...) */
+#define QS_ECUDA      -2   /* CUDA launch / runtime error                      */
+#define QS_EWORKSPACE -3   /* caller workspace too small                       */
+#define QS_ENOTSUP    -4   /* valid but unsupported configuration              */
+#define QS_ETIMEOUT   -5   /* a bounded device-side wait gave up               */
+
+/* ---- dtypes ------------------------------------------------------------ */
+#define QS_C64   0
+#define QS_C128  1
+
+/* ---- single-gate kinds (qs_apply_1q / qs_apply_2q) ----------------------- */
+#define QS_K_DENSE     0  /* full matrix                                       */
+#define QS_K_DIAG      1  /* diagonal; a leading 1 on the diagonal is skipped  */
+#define QS_K_ANTIDIAG  2  /* 1q only: v0' = m01*v1, v1' = m10*v0 (X, Y, CX ...) */
+#define QS_K_SWAP      3  /* 2q only: v01' = m12*v10, v10' = m21*v01, v00*=m00, v11*=m33 */
+
+/* ---- fused-pass op kinds ------------------------------------------------- */
+#define QS_OP_MAT   1     /* dense 2^m x 2^m on m tile-resident bits           */
+#define QS_OP_DIAG  2     /* diagonal on m bits anywhere in the vector         */
+
+/* ---- probability sources and sampling modes ------------------------------ */
+#define QS_SRC_SV  0      /* p_i = |vec[i]|^2                                  */
+#define QS_SRC_DM  1      /* p_i = Re rho[i, i] of a 2^n x 2^n density matrix  */
+#define QS_SAMPLE_CDF  0  /* one uniform per shot: smallest i with u <= CDF[i] */
+#define QS_SAMPLE_SEQ  1  /* n uniforms per shot, qubit 0 (MSB) first, outcome
+                             1 iff u > P(0) -- the reference's per-qubit rule  */
+
+#define QS_MAX_TILE_BITS 14
+#define QS_MAX_PASS_OPS  160
+
+/* One op of a fused pass.  64 bytes, plain old data (mirrored by ctypes). */
+typedef struct qs_op {
+    int32_t  kind;       /* QS_OP_MAT or QS_OP_DIAG                             */
+    int32_t  m;          /* number of target bits, 1..4                         */
+    int32_t  tgt[4];     /* tile-local position of target j, or -1 when the bit
+                            lies outside the tile (allowed for QS_OP_DIAG only) */
+    int32_t  gbit[4];    /* vector bit of target j (matrix-index bit m-1-j)     */
+    uint32_t lctrl;      /* control mask on tile-local positions                */
+    uint32_t pad0;
+    uint64_t gctrl;      /* control mask on vector bits outside the tile        */
+    int64_t  mat;        /* element offset of the op's matrix in the table
+                            (QS_OP_MAT: 4^m entries, QS_OP_DIAG: 2^m entries)   */
+} qs_op;
+
+/* One fused pass: a tile of 2^k amplitudes made of vector bits 0..nlow-1 and
+ * hi[0..k-nlow-1] (ascending), and ops [op_begin, op_begin+op_count). */
+typedef struct qs_pass {
+    int32_t k;
+    int32_t nlow;
+    int32_t hi[QS_MAX_TILE_BITS];
+    int32_t op_begin;
+    int32_t op_count;
+} qs_pass;
+
+/* ---- library ------------------------------------------------------------ */
+int         qs_version(void);
+const char* qs_last_error(void);
+/* Number of SMs of the current device (grid sizing; host query only). */
+int         qs_device_sm_count(void);
+
+/* ---- state preparation -------------------------------------------------- */
+/* vec <- |0...0> (replaces initial_state_vector, statevector_simulator.py:115-121). */
+int qs_init_zero(void* vec, int n, int dtype, void* stream);
+/* vec *= (re + i*im) (replaces float_multiply / complex_multiply,
+ * QuICT/ops/gate_kernel/multigpu_gate_func.py:13-102). */
+int qs_scale(void* vec, int n, int dtype, double re, double im, void* stream);
+
+/* ---- single gates --------------------------------------------------------- */
+/* One-target gate on `bit`, applied where all `ctrl_mask` bits are 1.
+ * mat: host complex128[4] (row-major 2x2).  Replaces, by kind:
+ *   DENSE    normal_targ, normal_ctargs           gate_function.py:1095-1119, 1236-1262
+ *   DIAG     diagonal_targ, control_targ, diagonal_ctargs, control_ctargs,
+ *            diagonal_more                         gate_function.py:1034-1058, 1151-1233, 1517-1552
+ *   ANTIDIAG swap_targ, reverse_targ, reverse_ctargs, reverse_more
+ *                                                  gate_function.py:1362-1442, 1479-1514 */
+int qs_apply_1q(void* vec, int n, int dtype, int bit, uint64_t ctrl_mask,
+                int kind, const double* mat, void* stream);
+
+/* Two-target gate; bit_hi carries matrix-index bit 1 (first argument), bit_lo
+ * matrix-index bit 0.  mat: host complex128[16].  Replaces
+ *   DENSE normal_targs, ctrl_normal_targs, normal_normal_targs,
+ *         diagonal_normal_targs                    gate_function.py:1122-1148, 1265-1359
+ *   DIAG  diagonal_targs                           gate_function.py:1061-1092
+ *   SWAP  swap_targs, swap_tmore                   gate_function.py:1445-1476, 1555-1590 */
+int qs_apply_2q(void* vec, int n, int dtype, int bit_hi, int bit_lo,
+                uint64_t ctrl_mask, int kind, const double* mat, void* stream);
+
+/* Dense k-target gate, 1 <= k <= 10, in place.  bits[j] carries matrix-index
+ * bit k-1-j.  mat_dev: DEVICE complex128[4^k].  Replaces matrix_dot_vector
+ * (QuICT/ops/linalg/gpu_calculator.py:343-478), which is out of place. */
+int qs_apply_kq(void* vec, int n, int dtype, int k, const int32_t* bits,
+                uint64_t ctrl_mask, const void* mat_dev, void* stream);
+
+/* ---- fused passes ---------------------------------------------------------- */
+/* Applies `npasses` passes; each pass is one launch that streams the vector
+ * through shared-memory tiles once and applies all of its ops per tile.
+ * passes / ops: HOST arrays (nops_total entries in ops); mats_dev: DEVICE
+ * table of mats_count complex entries in the state's dtype.  Every pass and op
+ * is validated on the host before the first launch.
+ * No reference counterpart: the reference launches one kernel per gate
+ * (statevector_simulator.py:155-164). */
+int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes, int npasses,
+                   const qs_op* ops, int64_t nops_total, const void* mats_dev,
+                   int64_t mats_count, void* stream);
+
+/* ---- measurement, reset, sampling ------------------------------------------ */
+size_t qs_reduce_ws_bytes(int n);
+/* *out_dev <- sum over {i : bit b of i is 0} of p_i, in FP64 (src = QS_SRC_*).
+ * Replaces measured_prob_calculate (gate_function.py:1751-1776). */
+int qs_prob0(const void* src, int n, int dtype, int src_kind, int bit,
+             void* ws, size_t ws_bytes, double* out_dev, void* stream);
+/* *out_dev <- sum_i p_i in FP64. */
+int qs_norm2(const void* src, int n, int dtype, int src_kind,
+             void* ws, size_t ws_bytes, double* out_dev, void* stream);
+/* Keep the `outcome` half of `bit`, scale it by `scale`, zero the other half.
+ * Replaces apply_measuregate's collapse (gate_function.py:1779-1815). */
+int qs_collapse(void* vec, int n, int dtype, int bit, int outcome, double scale, void* stream);
+/* Reset `bit` to |0> given P(0) = p0, with the reference's rule
+ * (gate_function.py:1818-1847; cpu_calculator.py:366-384). */
+int qs_reset(void* vec, int n, int dtype, int bit, double p0, void* stream);
+
+/* Sampling workspace: a sum tree of FP64 block sums. */
+size_t qs_sample_ws_bytes(int n);
+int qs_sample_prepare(const void* src, int n, int dtype, int src_kind,
+                      void* ws, size_t ws_bytes, void* stream);
+/* out_idx_dev[s] <- sampled basis index of shot s.  u_dev: DEVICE doubles,
+ * `shots` of them (QS_SAMPLE_CDF) or shots*n (QS_SAMPLE_SEQ, shot-major).
+ * Replaces the shots x qubits loop of StateVectorSimulator.sample
+ * (statevector_simulator.py:595-626). */
+int qs_sample(const void* src, int n, int dtype, int src_kind, const void* ws,
+              size_t ws_bytes, const double* u_dev, int64_t shots, int mode,
+              int64_t* out_idx_dev, void* stream);
+/* counts_dev[idx_dev[s]] += 1 (int64, caller zeroes counts_dev). */
+int qs_histogram(const int64_t* idx_dev, int64_t shots, int64_t* counts_dev,
+                 int64_t ncounts, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QSIM_H */

@@ -1,0 +1,136 @@
+"""ctypes binding of libqsim.so (the C-ABI declared in include/qsim.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+the shared object is missing or fails to load, every simulator entry point
+raises ``NativeLibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqsim.so")
+
+# ---- constants mirrored from include/qsim.h --------------------------------
+QS_OK, QS_EINVAL, QS_ECUDA, QS_EWORKSPACE, QS_ENOTSUP, QS_ETIMEOUT = 0, -1, -2, -3, -4, -5
+QS_C64, QS_C128 = 0, 1
+QS_K_DENSE, QS_K_DIAG, QS_K_ANTIDIAG, QS_K_SWAP = 0, 1, 2, 3
+QS_OP_MAT, QS_OP_DIAG = 1, 2
+QS_SRC_SV, QS_SRC_DM = 0, 1
+QS_SAMPLE_CDF, QS_SAMPLE_SEQ = 0, 1
+QS_MAX_TILE_BITS = 14
+QS_MAX_PASS_OPS = 160
+
+
+class NativeLibraryError(RuntimeError):
+    """libqsim.so is missing or could not be loaded."""
+
+
+class QsimError(RuntimeError):
+    """A libqsim call returned a negative status."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed ({code}): {msg}")
+        self.code = code
+
+
+class qs_op(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("m", C.c_int32),
+        ("tgt", C.c_int32 * 4),
+        ("gbit", C.c_int32 * 4),
+        ("lctrl", C.c_uint32),
+        ("pad0", C.c_uint32),
+        ("gctrl", C.c_uint64),
+        ("mat", C.c_int64),
+    ]
+
+
+class qs_pass(C.Structure):
+    _fields_ = [
+        ("k", C.c_int32),
+        ("nlow", C.c_int32),
+        ("hi", C.c_int32 * QS_MAX_TILE_BITS),
+        ("op_begin", C.c_int32),
+        ("op_count", C.c_int32),
+    ]
+
+
+assert C.sizeof(qs_op) == 64
+assert C.sizeof(qs_pass) == 8 + 4 * QS_MAX_TILE_BITS + 8
+
+_vp, _i, _i64, _u64, _d, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "qs_version": (_i, []),
+    "qs_last_error": (C.c_char_p, []),
+    "qs_device_sm_count": (_i, []),
+    "qs_init_zero": (_i, [_vp, _i, _i, _vp]),
+    "qs_scale": (_i, [_vp, _i, _i, _d, _d, _vp]),
+    "qs_apply_1q": (_i, [_vp, _i, _i, _i, _u64, _i, _dp, _vp]),
+    "qs_apply_2q": (_i, [_vp, _i, _i, _i, _i, _u64, _i, _dp, _vp]),
+    "qs_apply_kq": (_i, [_vp, _i, _i, _i, _i32p, _u64, _vp, _vp]),
+    "qs_apply_fused": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp]),
+    "qs_reduce_ws_bytes": (_sz, [_i]),
+    "qs_prob0": (_i, [_vp, _i, _i, _i, _i, _vp, _sz, _vp, _vp]),
+    "qs_norm2": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp, _vp]),
+    "qs_collapse": (_i, [_vp, _i, _i, _i, _i, _d, _vp]),
+    "qs_reset": (_i, [_vp, _i, _i, _i, _d, _vp]),
+    "qs_sample_ws_bytes": (_sz, [_i]),
+    "qs_sample_prepare": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp]),
+    "qs_sample": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp, _i64, _i, _vp, _vp]),
+    "qs_histogram": (_i, [_vp, _i64, _vp, _i64, _vp]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libqsim.so once; raise NativeLibraryError when it is unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NativeLibraryError(
+            f"{LIB_PATH} not found: build it with `python -m quict_b200.build` (no CPU fallback exists)"
+        )
+    try:
+        lib = C.CDLL(LIB_PATH)
+    except OSError as e:  # pragma: no cover - depends on the machine
+        raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> int:
+    """Call a status-returning entry point and raise QsimError on failure."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc < 0:
+        msg = lib.qs_last_error().decode(errors="replace")
+        raise QsimError(name, rc, msg)
+    return rc
+
+
+def mat_ptr(m: np.ndarray):
+    """Host complex128 matrix -> (keepalive array, double*)."""
+    a = np.ascontiguousarray(m, dtype=np.complex128)
+    return a, a.ctypes.data_as(_dp)
+
+
+def stream_ptr(stream) -> int | None:
+    """torch.cuda.Stream (or None) -> raw cudaStream_t value for ctypes."""
+    if stream is None:
+        return None
+    return int(stream.cuda_stream) or None

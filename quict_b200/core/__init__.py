@@ -1,0 +1,4 @@
+"""QuICT.core-compatible circuit IR (gates, circuits, noise) for the simulators."""
+from .gate import *  # noqa: F401,F403
+from .gate import BasicGate, GateType, MatrixType, UnitaryGate, QFTGate, PermGate, GATE_BY_NAME  # noqa: F401
+from .circuit import Circuit, Qubit, Qureg  # noqa: F401

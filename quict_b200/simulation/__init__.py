@@ -1,0 +1,2 @@
+"""Simulators: drop-in replacements for QuICT.simulation's GPU backends."""
+from .state_vector import StateVectorSimulator, StateArray  # noqa: F401

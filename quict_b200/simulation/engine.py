@@ -1,0 +1,190 @@
+"""Device engine: runs lowered ops on a torch-owned state through libqsim.
+
+Torch is the allocator and the stream provider; every kernel launch goes
+through the C-ABI in ``quict_b200._native``.  There is no CPU path: a missing
+CUDA device or library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from .fusion import MatrixTable, Pass, Single, default_tile, emit, fusable, plan
+from .lowering import Op
+
+DTYPES = {
+    np.complex64: (torch.complex64, N.QS_C64, 8),
+    np.complex128: (torch.complex128, N.QS_C128, 16),
+}
+
+
+def qs_dtype(t: torch.Tensor) -> int:
+    if t.dtype == torch.complex128:
+        return N.QS_C128
+    if t.dtype == torch.complex64:
+        return N.QS_C64
+    raise TypeError(f"state must be complex64 or complex128, got {t.dtype}")
+
+
+def require_cuda(device_id: int = 0) -> torch.device:
+    N.load()
+    if not torch.cuda.is_available():
+        raise RuntimeError("quict_b200 simulators need a CUDA device; none is visible (no CPU fallback)")
+    return torch.device("cuda", device_id)
+
+
+class Workspace:
+    """Grow-only device scratch owned by torch; handed to libqsim as (ptr, bytes)."""
+
+    def __init__(self, device: torch.device):
+        self.device = device
+        self.buf: Optional[torch.Tensor] = None
+
+    def get(self, nbytes: int) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self.buf
+
+
+class Engine:
+    def __init__(self, device: torch.device, fusion: bool = True, tile_bits: Optional[int] = None,
+                 low_bits: Optional[int] = None, max_pass_cost: float = float("inf")):
+        self.device = device
+        self.fusion = fusion
+        self.tile_bits = tile_bits
+        self.low_bits = low_bits
+        self.max_pass_cost = max_pass_cost
+        self.ws = Workspace(device)
+        self.launches = 0  # libqsim kernel launches issued (per gate or per fused pass)
+        self.h2d_bytes = 0  # host->device bytes copied for matrix tables
+        self.pass_events = None  # list -> record (start, end, nops) CUDA events per fused pass
+
+    @property
+    def stream(self):
+        return N.stream_ptr(torch.cuda.current_stream(self.device))
+
+    # ---- per-gate path -------------------------------------------------------------
+    def apply_single(self, vec: torch.Tensor, n: int, op: Op):
+        dt = qs_dtype(vec)
+        ptr = C.c_void_p(vec.data_ptr())
+        cmask = 0
+        for b in op.cbits:
+            cmask |= 1 << b
+        st = self.stream
+        if op.m >= 3:
+            d = op.dense()
+            dm = torch.from_numpy(np.ascontiguousarray(d, dtype=np.complex128)).to(self.device, non_blocking=False)
+            bits = (C.c_int32 * op.m)(*op.tbits)
+            N.call("qs_apply_kq", ptr, n, dt, op.m, bits, cmask, C.c_void_p(dm.data_ptr()), st)
+            self._keep = dm
+        elif op.m == 1:
+            kind = {"mat": N.QS_K_DENSE, "diag": N.QS_K_DIAG, "antidiag": N.QS_K_ANTIDIAG}[op.kind]
+            keep, mp = N.mat_ptr(op.dense())
+            N.call("qs_apply_1q", ptr, n, dt, op.tbits[0], cmask, kind, mp, st)
+        elif op.m == 2:
+            kind = {"mat": N.QS_K_DENSE, "diag": N.QS_K_DIAG, "swap": N.QS_K_SWAP}[op.kind]
+            keep, mp = N.mat_ptr(op.dense())
+            N.call("qs_apply_2q", ptr, n, dt, op.tbits[0], op.tbits[1], cmask, kind, mp, st)
+        else:
+            raise ValueError(f"cannot apply op kind {op.kind} with {op.m} targets")
+        self.launches += 1
+
+    # ---- fused path -------------------------------------------------------------------
+    def tile_shape(self, vec: torch.Tensor):
+        k0, l0 = default_tile(vec.element_size())
+        return (self.tile_bits or k0), (self.low_bits if self.low_bits is not None else l0)
+
+    def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        k, nlow = self.tile_shape(vec)
+        return plan(ops, n, k, nlow, max_cost=self.max_pass_cost)
+
+    def run_passes(self, vec: torch.Tensor, n: int, passes: List[Pass]):
+        if not passes:
+            return
+        table = MatrixTable()
+        cps, npass, cops, nops = emit(passes, table)
+        host = table.array().astype(np.complex64 if vec.dtype == torch.complex64 else np.complex128)
+        mats = torch.from_numpy(host).to(self.device)
+        self.h2d_bytes += mats.numel() * mats.element_size()
+        if self.pass_events is None:
+            N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), cps, npass, cops, nops,
+                   C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+        else:
+            # one call per pass, bracketed by CUDA events on the launching stream
+            stream = torch.cuda.current_stream(self.device)
+            for i in range(npass):
+                if passes[i].ops:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), C.byref(cps[i]), 1,
+                       cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+                if passes[i].ops:
+                    b.record(stream)
+                    self.pass_events.append((a, b, len(passes[i].ops)))
+        self._keep = mats
+        self.launches += sum(1 for p in passes if p.ops)
+
+    def apply_ops(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        """Apply unitary ops (no measure/reset/perm) in order."""
+        if not self.fusion:
+            for op in ops:
+                self.apply_single(vec, n, op)
+            return
+        batch: List[Pass] = []
+        for step in self.plan(vec, n, ops):
+            if isinstance(step, Pass):
+                batch.append(step)
+            else:
+                self.run_passes(vec, n, batch)
+                batch = []
+                self.apply_single(vec, n, step.op)
+        self.run_passes(vec, n, batch)
+
+    # ---- reductions / measurement -------------------------------------------------------
+    def prob0(self, src: torch.Tensor, n: int, bit: int, src_kind: int = N.QS_SRC_SV) -> float:
+        ws = self.ws.get(N.load().qs_reduce_ws_bytes(n))
+        res = torch.empty(1, dtype=torch.float64, device=self.device)
+        N.call("qs_prob0", C.c_void_p(src.data_ptr()), n, qs_dtype(src), src_kind, bit,
+               C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(res.data_ptr()), self.stream)
+        return float(res.item())
+
+    def norm2(self, src: torch.Tensor, n: int, src_kind: int = N.QS_SRC_SV) -> float:
+        ws = self.ws.get(N.load().qs_reduce_ws_bytes(n))
+        res = torch.empty(1, dtype=torch.float64, device=self.device)
+        N.call("qs_norm2", C.c_void_p(src.data_ptr()), n, qs_dtype(src), src_kind,
+               C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(res.data_ptr()), self.stream)
+        return float(res.item())
+
+    def collapse(self, vec: torch.Tensor, n: int, bit: int, outcome: int, scale: float):
+        N.call("qs_collapse", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), bit, int(outcome), float(scale),
+               self.stream)
+
+    def reset(self, vec: torch.Tensor, n: int, bit: int, p0: float):
+        N.call("qs_reset", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), bit, float(p0), self.stream)
+
+    def sample_indices(self, src: torch.Tensor, n: int, uniforms: torch.Tensor, mode: int,
+                       src_kind: int = N.QS_SRC_SV) -> torch.Tensor:
+        """Device int64 tensor of sampled basis indices (one per shot)."""
+        lib = N.load()
+        wsb = lib.qs_sample_ws_bytes(n)
+        ws = self.ws.get(wsb)
+        u = uniforms.to(device=self.device, dtype=torch.float64).contiguous()
+        shots = u.numel() if mode == N.QS_SAMPLE_CDF else u.numel() // n
+        out = torch.empty(max(shots, 1), dtype=torch.int64, device=self.device)
+        st = self.stream
+        N.call("qs_sample_prepare", C.c_void_p(src.data_ptr()), n, qs_dtype(src), src_kind,
+               C.c_void_p(ws.data_ptr()), ws.numel(), st)
+        N.call("qs_sample", C.c_void_p(src.data_ptr()), n, qs_dtype(src), src_kind, C.c_void_p(ws.data_ptr()),
+               ws.numel(), C.c_void_p(u.data_ptr()), shots, mode, C.c_void_p(out.data_ptr()), st)
+        return out[:shots]
+
+    def histogram(self, idx: torch.Tensor, ncounts: int) -> torch.Tensor:
+        counts = torch.zeros(ncounts, dtype=torch.int64, device=self.device)
+        N.call("qs_histogram", C.c_void_p(idx.data_ptr()), idx.numel(), C.c_void_p(counts.data_ptr()), ncounts,
+               self.stream)
+        return counts

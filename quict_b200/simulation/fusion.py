@@ -1,0 +1,196 @@
+"""Fusion planner: groups a gate sequence into shared-memory tile passes.
+
+A pass keeps a tile of 2^k amplitudes on chip: vector bits 0..nlow-1 (so each
+warp streams contiguous 2^nlow-amplitude runs) plus k - nlow chosen higher
+bits.  An op joins the current pass when
+
+  * its non-diagonal targets (``Op.xbits``) fit into the tile, and
+  * it commutes with every op deferred so far.
+
+Two ops commute whenever every bit they share is a control or a diagonal
+target of both (each is then block-diagonal over those bits, acting on
+disjoint remaining bits), so diagonal gates (Rz, Rzz, CZ, phases) and controls
+never occupy tile bits and can be hoisted past unrelated work.  Ops that
+cannot be fused (dense on more than 4 bits, measurement, permutation) are
+returned as ``single`` steps that run with the per-gate kernels.
+
+The reference has no counterpart: it launches one kernel per gate
+(statevector_simulator.py:155-164).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, List, Sequence, Tuple, Union
+
+import numpy as np
+
+from .. import _native as N
+from .lowering import Op
+
+MAX_FUSED_M = 4
+
+
+@dataclass
+class Pass:
+    k: int
+    nlow: int
+    hi: Tuple[int, ...]
+    ops: List[Op] = field(default_factory=list)
+
+
+@dataclass
+class Single:
+    op: Op
+
+
+Step = Union[Pass, Single]
+
+
+def fusable(op: Op) -> bool:
+    return op.kind in ("mat", "diag", "antidiag", "swap") and op.m <= MAX_FUSED_M
+
+
+def default_tile(dtype_bytes: int) -> Tuple[int, int]:
+    """(k, nlow) giving a 64 KiB tile with 512-byte contiguous warp runs."""
+    k = 12 if dtype_bytes == 16 else 13
+    nlow = 5
+    return k, nlow
+
+
+def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_PASS_OPS,
+         max_cost: float = float("inf")) -> List[Step]:
+    """Greedy in-order planner with commutation-aware hoisting.
+
+    ``max_cost`` bounds the per-pass arithmetic, measured in dense-1q-gate
+    equivalents (see ``op_cost``), so that a pass stays bandwidth-bound.
+    """
+    k = min(k, n)
+    nlow = min(nlow, k)
+    H = k - nlow
+    low = frozenset(range(nlow))
+    steps: List[Step] = []
+    pending = list(ops)
+    def fits(op: Op) -> bool:
+        return fusable(op) and len(op.xbits - low) <= H
+
+    while pending:
+        # leading ops that can never be tile-resident run on their own
+        if not fits(pending[0]):
+            steps.append(Single(pending.pop(0)))
+            continue
+        hi: set = set()
+        chosen: List[Op] = []
+        deferred: List[Op] = []
+        xblk: set = set()
+        zblk: set = set()
+        cost = 0.0
+        stop = False
+        for idx, op in enumerate(pending):
+            if stop:
+                deferred.append(op)
+                continue
+            if not fits(op):
+                # a barrier: nothing after it may be hoisted above it
+                deferred.append(op)
+                stop = True
+                continue
+            xb, zb = op.xbits, op.zbits
+            allb = xb | zb
+            hoistable = not (allb & xblk) and not (xb & zblk)
+            need = xb - low - hi
+            c = op_cost(op)
+            if (hoistable and len(hi) + len(need) <= H and len(chosen) < max_ops
+                    and (cost + c <= max_cost or not chosen)):
+                hi |= need
+                chosen.append(op)
+                cost += c
+            else:
+                deferred.append(op)
+                xblk |= xb
+                zblk |= zb
+        # fill unused tile bits with the lowest free bits (longer contiguous runs)
+        b = nlow
+        while len(hi) < H:
+            if b not in hi:
+                hi.add(b)
+            b += 1
+        steps.append(Pass(k, nlow, tuple(sorted(hi)), chosen))
+        pending = deferred
+    return steps
+
+
+def op_cost(op: Op) -> float:
+    """Arithmetic of an op per amplitude, in units of a dense 1q gate (2 complex MACs)."""
+    if op.kind == "diag":
+        return 0.5
+    if op.kind in ("antidiag", "swap"):
+        return 0.5 * (1 << op.m) / 2
+    return (1 << op.m) / 2.0
+
+
+class MatrixTable:
+    """De-duplicated matrix table for one run (the role of GateMatrixs,
+    QuICT/simulation/utils/gate_based.py:38-101): matrices are keyed by content,
+    concatenated, and copied to the device once."""
+
+    def __init__(self):
+        self._chunks: List[np.ndarray] = []
+        self._index: Dict[bytes, int] = {}
+        self.size = 0
+
+    def add(self, entries: np.ndarray) -> int:
+        a = np.ascontiguousarray(entries, dtype=np.complex128).ravel()
+        key = a.tobytes()
+        off = self._index.get(key)
+        if off is None:
+            off = self.size
+            self._index[key] = off
+            self._chunks.append(a)
+            self.size += a.size
+        return off
+
+    def array(self) -> np.ndarray:
+        if not self._chunks:
+            return np.zeros(1, dtype=np.complex128)
+        return np.concatenate(self._chunks)
+
+
+def emit(passes: Sequence[Pass], table: MatrixTable):
+    """Convert passes into ctypes (qs_pass[], qs_op[]) arrays, filling `table`."""
+    cps = (N.qs_pass * max(1, len(passes)))()
+    nops = sum(len(p.ops) for p in passes)
+    cops = (N.qs_op * max(1, nops))()
+    o = 0
+    for pi, p in enumerate(passes):
+        cp = cps[pi]
+        cp.k, cp.nlow = p.k, p.nlow
+        for j, h in enumerate(p.hi):
+            cp.hi[j] = h
+        cp.op_begin, cp.op_count = o, len(p.ops)
+        local = {b: b for b in range(p.nlow)}
+        for j, h in enumerate(p.hi):
+            local[h] = p.nlow + j
+        for op in p.ops:
+            c = cops[o]
+            o += 1
+            c.m = op.m
+            for j, b in enumerate(op.tbits):
+                c.gbit[j] = b
+                c.tgt[j] = local.get(b, -1)
+            for j in range(op.m, 4):
+                c.gbit[j] = 0
+                c.tgt[j] = -1
+            lc, gc = 0, 0
+            for b in op.cbits:
+                if b in local:
+                    lc |= 1 << local[b]
+                else:
+                    gc |= 1 << b
+            c.lctrl, c.gctrl = lc, gc
+            if op.kind == "diag":
+                c.kind = N.QS_OP_DIAG
+                c.mat = table.add(op.mat)
+            else:
+                c.kind = N.QS_OP_MAT
+                c.mat = table.add(op.dense())
+    return cps, len(passes), cops, nops

@@ -1,0 +1,57 @@
+"""Seeded synthetic circuits with the shapes of the benchmark configurations.
+
+config0: n qubits, gates uniform over {H, X, Rx, Ry, Rz, U3, CX, CZ, Rzz,
+         Swap}, angles uniform in [0, 2 pi), distinct uniform qubits.
+config1: the same gate set plus 10% random Haar 2-qubit unitaries; every
+         qubit argument is drawn, with probability 1/2 each, from the qubits on
+         vector bits < 5 or from those on vector bits >= n - 10 (targets spread
+         over low and high bits).
+All generators use numpy.random.default_rng(seed); nothing is read from disk.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .core import GATE_BY_NAME, Circuit, Unitary
+
+CFG_GATES = ["h", "x", "rx", "ry", "rz", "u3", "cx", "cz", "rzz", "swap"]
+
+
+def haar_unitary(rng: np.random.Generator, d: int) -> np.ndarray:
+    """Haar-random d x d unitary (QR of a complex Ginibre matrix, phases fixed)."""
+    z = (rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))) / np.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def config0_circuit(n: int = 20, size: int = 200, seed: int = 0) -> Circuit:
+    c = Circuit(n)
+    c.random_append(size, seed=seed)
+    return c
+
+
+def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: float = 0.1) -> Circuit:
+    rng = np.random.default_rng(seed)
+    c = Circuit(n)
+    low = [n - 1 - b for b in range(min(5, n))]                 # qubits on vector bits 0..4
+    high = [n - 1 - b for b in range(max(5, n - 10), n)]        # qubits on vector bits >= n-10
+
+    def pick(k):
+        out = []
+        while len(out) < k:
+            grp = low if rng.random() < 0.5 else high
+            q = int(grp[rng.integers(len(grp))])
+            if q not in out:
+                out.append(q)
+        return out
+
+    for _ in range(size):
+        if rng.random() < haar_frac:
+            Unitary(haar_unitary(rng, 4)) | c(pick(2))
+            continue
+        nm = CFG_GATES[rng.integers(len(CFG_GATES))]
+        g = GATE_BY_NAME[nm]
+        if g.params:
+            g = g(*[float(x) for x in rng.uniform(0, 2 * np.pi, g.params)])
+        g | c(pick(g.controls + g.targets))
+    return c

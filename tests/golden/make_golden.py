@@ -1,0 +1,287 @@
+"""Generate the golden fixtures in tests/golden/ by running the REFERENCE
+(taofei95/quict) CPU simulators in this container.
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+The reference is imported with stub modules for its plotting / QASM-lexer
+dependencies (matplotlib, IPython, ply, pylatexenc, prettytable), which are
+off the arithmetic path, and with numpy.complex restored (removed in numpy 2,
+used in an annotation at statevector_simulator.py:525).  Only derived data is
+written: gate lists, amplitudes, density matrices, counts and the uniforms the
+reference consumed.  Nothing under /root/reference is copied.
+
+Fixtures
+  gates.json          matrix / matrix_type / arity of every reference gate type
+  qasm_circuit.json   random_circuit_for_correction.qasm as a gate list
+  qasm_state.npy      the reference's own golden state_vector.npy (10 qubits)
+  random_sv.npz       config-0 style random circuits (n=5, 8, 11), reference
+                      CPU StateVectorSimulator, double and single precision
+  ext_sv.npz          every gate family incl. 3-qubit gates (n=6): reference
+                      SV and reference UnitarySimulator
+  haar_sv.npz         random Haar 2q unitaries: reference SV (reversed order)
+                      and reference UnitarySimulator (big-endian)
+  sample.npz          reference CPU sample() counts with the numba-RNG uniforms
+  midmeasure.npz      Measure / Reset inside a circuit with recorded uniforms
+  dm.npz              reference DensityMatrixSimulator with noise (n=3, 4)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CFG0 = ["h", "x", "rx", "ry", "rz", "u3", "cx", "cz", "rzz", "swap"]
+EXT = ["h", "hy", "s", "sdg", "x", "y", "z", "sx", "sy", "sw", "u1", "u2", "u3", "rx", "ry", "rz", "t", "tdg",
+       "phase", "gphase", "cz", "cx", "cy", "ch", "crz", "cu1", "cu3", "fsim", "rxx", "ryy", "rzz", "rzx",
+       "swap", "iswap", "iswapdg", "ccx", "ccz", "ccrz", "cswap"]
+
+
+def shim(ref: str):
+    np.complex = complex  # type: ignore[attr-defined]
+    names = ["matplotlib", "matplotlib.pyplot", "matplotlib.patches", "matplotlib.path", "matplotlib.lines",
+             "matplotlib.text", "matplotlib.figure", "matplotlib.collections", "matplotlib.transforms",
+             "matplotlib.colors", "IPython", "IPython.display", "ply", "ply.lex", "ply.yacc", "pylatexenc",
+             "pylatexenc.latexencode", "prettytable"]
+    for name in names:
+        m = types.ModuleType(name)
+        m.__path__ = []
+
+        def _ga(attr, _n=name):
+            if attr[:1].islower():
+                return lambda *a, **k: None
+            return type(attr, (), {"__init__": lambda self, *a, **k: None})
+
+        m.__getattr__ = _ga
+        sys.modules[name] = m
+    sys.path.insert(0, ref)
+
+
+def gate_list_random(rng, n, size, names):
+    out = []
+    from QuICT.core.gate import GATE_TYPE_TO_CLASS, GateType
+    for _ in range(size):
+        nm = names[rng.integers(len(names))]
+        g = GATE_TYPE_TO_CLASS[GateType.__members__[nm]]()
+        k = g.controls + g.targets
+        args = [int(a) for a in rng.choice(n, k, replace=False)]
+        params = [float(rng.uniform(0, 2 * np.pi)) for _ in range(g.params)]
+        out.append([nm, args, params])
+    return out
+
+
+def build(gl, n, precision="double"):
+    from QuICT.core import Circuit
+    from QuICT.core.gate import GATE_TYPE_TO_CLASS, GateType
+    c = Circuit(n)
+    for nm, args, params in gl:
+        if nm == "unitary":
+            from QuICT.core.gate import Unitary
+            g = Unitary(np.array(params, dtype=np.complex128))
+        else:
+            g = GATE_TYPE_TO_CLASS[GateType.__members__[nm]]()
+            if params:
+                g = g(*params)
+        g | c(list(args))
+    if precision == "single":
+        c.convert_precision()
+    return c
+
+
+def sv_cpu(c, precision="double"):
+    from QuICT.simulation.state_vector import StateVectorSimulator
+    return np.asarray(StateVectorSimulator(device="CPU", precision=precision).run(c)).copy()
+
+
+def unitary_cpu(c):
+    from QuICT.simulation.unitary import UnitarySimulator
+    return np.asarray(UnitarySimulator(device="CPU").run(c)).copy()
+
+
+def parse_qasm(path):
+    gl, n = [], None
+    for line in open(path):
+        line = line.strip()
+        if not line or line.startswith(("OPENQASM", "include", "creg")):
+            continue
+        m = re.match(r"qreg\s+\w+\[(\d+)\];", line)
+        if m:
+            n = int(m.group(1))
+            continue
+        m = re.match(r"(\w+)(?:\(([^)]*)\))?\s+(.*);", line)
+        name, ps, qs = m.group(1), m.group(2), m.group(3)
+        params = [float(eval(p, {"pi": np.pi})) for p in ps.split(",")] if ps else []
+        args = [int(x) for x in re.findall(r"\[(\d+)\]", qs)]
+        gl.append([name, args, params])
+    return n, gl
+
+
+def haar(rng, d):
+    z = (rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))) / np.sqrt(2)
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    shim(a.ref)
+    from QuICT.core.gate import GATE_TYPE_TO_CLASS, GateType
+
+    # ---- gate matrices ---------------------------------------------------------------
+    rng = np.random.default_rng(7)
+    gates = {}
+    for nm in EXT + ["id"]:
+        g = GATE_TYPE_TO_CLASS[GateType.__members__[nm]]()
+        params = [float(rng.uniform(0, 2 * np.pi)) for _ in range(g.params)]
+        if params:
+            g = g(*params)
+        m = np.asarray(g.matrix, dtype=np.complex128)
+        gates[nm] = {"controls": g.controls, "targets": g.targets, "params": params,
+                     "matrix_type": g.matrix_type.name, "re": m.real.tolist(), "im": m.imag.tolist()}
+    json.dump(gates, open(os.path.join(HERE, "gates.json"), "w"))
+
+    # ---- the reference's own golden circuit ---------------------------------------------
+    qasm = os.path.join(a.ref, "unit_test/simulation/data/random_circuit_for_correction.qasm")
+    n, gl = parse_qasm(qasm)
+    golden = np.load(os.path.join(a.ref, "unit_test/simulation/data/state_vector.npy"))
+    ours = sv_cpu(build(gl, n))
+    assert np.allclose(ours, golden, atol=1e-12), "reference CPU SV does not reproduce its golden vector"
+    json.dump({"n": n, "gates": gl}, open(os.path.join(HERE, "qasm_circuit.json"), "w"))
+    np.save(os.path.join(HERE, "qasm_state.npy"), golden)
+
+    # ---- random config-0 circuits ---------------------------------------------------------
+    out = {}
+    for n, size, seed in [(5, 40, 11), (8, 80, 12), (11, 120, 13)]:
+        rng = np.random.default_rng(seed)
+        gl = gate_list_random(rng, n, size, CFG0)
+        out[f"n{n}_gates"] = np.array(json.dumps(gl))
+        out[f"n{n}_double"] = sv_cpu(build(gl, n))
+        out[f"n{n}_single"] = sv_cpu(build(gl, n, "single"), "single")
+    np.savez_compressed(os.path.join(HERE, "random_sv.npz"), **out)
+
+    # ---- every gate family ----------------------------------------------------------------
+    # Two circuits, each avoiding one reference inconsistency:
+    #  * the CPU SV path applies iSwap-family gates as plain swaps
+    #    (swap_matrix ignores the matrix, cpu_calculator.py:238-280), so the
+    #    SV circuit "a" has no iswap / iswapdg;
+    #  * UnitarySimulator's CircuitMatrix applies Rzx with reversed arguments
+    #    in some gate contexts only, so the Unitary circuit "b" has no rzx.
+    from QuICT.simulation.unitary import UnitarySimulator
+    out = {}
+    n = 6
+    rng = np.random.default_rng(21)
+    ga = [["h", [q], []] for q in range(n)] + gate_list_random(
+        rng, n, 160, [x for x in EXT if x not in ("iswap", "iswapdg")])
+    out["a_gates"] = np.array(json.dumps(ga))
+    out["a_sv"] = sv_cpu(build(ga, n))
+    rng = np.random.default_rng(22)
+    gb = [["h", [q], []] for q in range(n)] + gate_list_random(rng, n, 160, [x for x in EXT if x != "rzx"])
+    out["b_gates"] = np.array(json.dumps(gb))
+    out["b_unitary"] = np.asarray(UnitarySimulator(device="CPU").run(build(gb, n))).copy()
+    np.savez_compressed(os.path.join(HERE, "ext_sv.npz"), **out)
+
+    # ---- Haar 2q unitaries --------------------------------------------------------------------
+    out = {}
+    rng = np.random.default_rng(31)
+    n = 5
+    gl = [["h", [q], []] for q in range(n)]
+    for _ in range(12):
+        args = [int(x) for x in rng.choice(n, 2, replace=False)]
+        m = haar(rng, 4)
+        gl.append(["unitary", args, m.tolist()])
+        gl.append(["rx", [int(rng.integers(n))], [float(rng.uniform(0, 2 * np.pi))]])
+    ser = [[nm, args, ([[complex(x).real, complex(x).imag] for x in np.ravel(p)] if nm == "unitary" else p)]
+           for nm, args, p in gl]
+    out["gates"] = np.array(json.dumps(ser))
+    out["sv_reference"] = sv_cpu(build(gl, n))
+    out["unitary_reference"] = np.asarray(UnitarySimulator(device="CPU").run(build(gl, n))).copy()
+    np.savez_compressed(os.path.join(HERE, "haar_sv.npz"), **out)
+
+    # ---- sampling with the reference's numba RNG --------------------------------------------------
+    import numba
+    import random
+
+    @numba.njit
+    def nb_seed(s):
+        random.seed(s)
+
+    @numba.njit
+    def nb_draw(k):
+        r = np.empty(k)
+        for i in range(k):
+            r[i] = random.random()
+        return r
+
+    from QuICT.simulation.state_vector import StateVectorSimulator
+    out = {}
+    for n, shots, seed in [(4, 300, 101), (6, 200, 102)]:
+        rng = np.random.default_rng(seed)
+        gl = gate_list_random(rng, n, 6 * n, CFG0)
+        c = build(gl, n)
+        sim = StateVectorSimulator(device="CPU")
+        sv = np.asarray(sim.run(c)).copy()
+        nb_seed(seed)
+        u = nb_draw(shots * n)
+        nb_seed(seed)
+        counts = np.asarray(sim.sample(shots), dtype=np.int64)
+        out[f"n{n}_gates"] = np.array(json.dumps(gl))
+        out[f"n{n}_state"] = sv
+        out[f"n{n}_uniforms"] = u
+        out[f"n{n}_counts"] = counts
+    np.savez_compressed(os.path.join(HERE, "sample.npz"), **out)
+
+    # ---- measure / reset inside a circuit --------------------------------------------------------
+    out = {}
+    n = 5
+    rng = np.random.default_rng(202)
+    gl = gate_list_random(rng, n, 20, CFG0)
+    gl += [["measure", [1], []], ["reset", [3], []]]
+    gl += gate_list_random(rng, n, 10, CFG0)
+    gl += [["measure", [4], []], ["reset", [0], []], ["measure", [2], []]]
+    c = build(gl, n)
+    nb_seed(303)
+    u = nb_draw(8)
+    nb_seed(303)
+    sim = StateVectorSimulator(device="CPU")
+    sv = np.asarray(sim.run(c)).copy()
+    out["gates"] = np.array(json.dumps(gl))
+    out["uniforms"] = u
+    out["state"] = sv
+    out["measured"] = np.array([c.qubits[q].measured if c.qubits[q].measured is not None else -1
+                                for q in range(n)])
+    np.savez_compressed(os.path.join(HERE, "midmeasure.npz"), **out)
+
+    # ---- noisy density matrix ------------------------------------------------------------------------
+    from QuICT.core.noise import NoiseModel, DepolarizingError, DampingError
+    from QuICT.simulation.density_matrix import DensityMatrixSimulator
+    out = {}
+    for n, size, seed in [(3, 10, 401), (4, 14, 402)]:
+        rng = np.random.default_rng(seed)
+        gl = gate_list_random(rng, n, size, ["h", "u3", "rx", "rzz", "swap", "cx", "cz"])
+        amp1 = DampingError(amplitude_prob=5e-3, phase_prob=0)
+        e1 = amp1.compose(DepolarizingError(1e-3, 1))
+        e2 = amp1.tensor(amp1).compose(DepolarizingError(1e-2, 2))
+        nm = NoiseModel(basic_gates=["h", "u3", "rx", "rzz", "swap", "cx", "cz"])
+        nm.add_noise_for_all_qubits(e1, ["h", "u3", "rx"])
+        nm.add_noise_for_all_qubits(e2, ["rzz", "swap", "cx", "cz"])
+        dm = DensityMatrixSimulator(device="CPU", accumulated_mode=True).run(build(gl, n), noise_model=nm)
+        clean = DensityMatrixSimulator(device="CPU").run(build(gl, n))
+        out[f"n{n}_gates"] = np.array(json.dumps(gl))
+        out[f"n{n}_noisy"] = np.asarray(dm).copy()
+        out[f"n{n}_clean"] = np.asarray(clean).copy()
+        out[f"n{n}_kraus1"] = np.array([np.asarray(k) for k in e1.kraus])
+        out[f"n{n}_kraus2"] = np.array([np.asarray(k) for k in e2.kraus])
+    np.savez_compressed(os.path.join(HERE, "dm.npz"), **out)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

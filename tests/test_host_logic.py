@@ -1,0 +1,185 @@
+"""Host-side logic on CPU: lowering, fusion planning, C-ABI exports and
+argument validation (no kernel runs)."""
+import ctypes as C
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, build_circuit, golden, oracle_gates
+from oracle import sv as osv
+
+
+def _apply_ops_oracle(vec, n, ops):
+    """Apply lowered Ops with the oracle (vector bits -> circuit qubits)."""
+    for op in ops:
+        args = [n - 1 - b for b in op.cbits] + [n - 1 - b for b in op.tbits]
+        u = op.dense()
+        d = 1 << len(op.cbits)
+        if d > 1:
+            full = np.eye(u.shape[0] * d, dtype=np.complex128)
+            full[-u.shape[0]:, -u.shape[0]:] = u
+            u = full
+        vec = osv.apply_matrix(vec, n, u, args)
+    return vec
+
+
+def _all_ops(n, seed, size=120):
+    from quict_b200.simulation.lowering import lower_circuit
+    d = golden("ext_sv.npz")
+    gl = json.loads(str(d["b_gates"]))
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(6)
+    gl = [[nm, [int(perm[a]) for a in args], p] for nm, args, p in gl][:size]
+    c = build_circuit(gl, 6)
+    return c, lower_circuit(c.gates, 6)
+
+
+def test_lowering_reproduces_circuit():
+    c, ops = _all_ops(6, 0)
+    ref = osv.run(oracle_gates(c), 6)
+    got = _apply_ops_oracle(osv.zero_state(6), 6, ops)
+    np.testing.assert_allclose(got, ref, atol=1e-12)
+    kinds = {o.kind for o in ops}
+    assert kinds >= {"mat", "diag", "antidiag", "swap"}
+
+
+def test_lowering_kinds_and_controls():
+    from quict_b200.core import CX, CZ, Rz, Rzz, Swap, H, CCX, sqiSwap
+    from quict_b200.simulation.lowering import lower_gate
+    n = 5
+    (op,) = lower_gate(CX & [0, 3], n)
+    assert op.kind == "antidiag" and op.cbits == (4,) and op.tbits == (1,)
+    (op,) = lower_gate(CZ & [2, 1], n)
+    assert op.kind == "diag" and op.cbits == (2,) and op.tbits == (3,)
+    (op,) = lower_gate(Rzz(0.3) & [0, 4], n)
+    assert op.kind == "diag" and op.tbits == (4, 0) and op.cbits == ()
+    (op,) = lower_gate(Swap & [1, 2], n)
+    assert op.kind == "swap"
+    (op,) = lower_gate(CCX & [0, 1, 2], n)
+    assert op.kind == "antidiag" and set(op.cbits) == {4, 3}
+    (op,) = lower_gate(sqiSwap & [0, 1], n)  # typed "swap" by QuICT, but not a pure swap
+    assert op.kind == "mat"
+    assert lower_gate(Rz(0.0) & 1, n) == []   # identity is skipped
+
+
+def test_legacy_order_reverses_only_uncontrolled_dense():
+    from quict_b200.core import Unitary, CH, Rzz
+    from quict_b200.simulation.lowering import lower_gate
+    m = np.arange(16).reshape(4, 4) + 1j
+    (a,) = lower_gate(Unitary(m) & [0, 2], 4, legacy_2q_order=True)
+    (b,) = lower_gate(Unitary(m) & [0, 2], 4)
+    assert a.tbits == b.tbits[::-1]
+    (c,) = lower_gate(CH & [0, 2], 4, legacy_2q_order=True)
+    assert c.cbits == (3,) and c.tbits == (1,)
+    (d,) = lower_gate(Rzz(0.4) & [0, 2], 4, legacy_2q_order=True)
+    assert d.tbits == (3, 1)
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("k,nlow", [(3, 1), (4, 2), (5, 5), (4, 0)])
+def test_fusion_plan_preserves_semantics(seed, k, nlow):
+    """Executing the planner's passes in order equals the original order."""
+    from quict_b200.simulation.fusion import Pass, Single, plan
+    c, ops = _all_ops(6, seed)
+    steps = plan(ops, 6, k, nlow, max_ops=7)
+    flat = []
+    for s in steps:
+        if isinstance(s, Pass):
+            tile = set(range(min(nlow, k))) | set(s.hi)
+            assert len(tile) == min(k, 6)
+            for op in s.ops:
+                assert op.xbits <= tile
+            flat.extend(s.ops)
+        else:
+            flat.append(s.op)
+    assert sorted(map(id, flat)) == sorted(map(id, ops))
+    ref = _apply_ops_oracle(osv.zero_state(6), 6, ops)
+    got = _apply_ops_oracle(osv.zero_state(6), 6, flat)
+    np.testing.assert_allclose(got, ref, atol=1e-12)
+
+
+def test_fusion_hoists_diagonal_and_controls():
+    from quict_b200.core import Circuit, H, Rz, CZ, CX, Rzz
+    from quict_b200.simulation.fusion import plan
+    from quict_b200.simulation.lowering import lower_circuit
+    n = 20
+    c = Circuit(n)
+    for q in range(n):
+        Rz(0.1 * q) | c(q)
+    for q in range(n - 1):
+        CZ | c([q, q + 1])
+        Rzz(0.2) | c([q, q + 1])
+    for q in range(10, 20):
+        H | c(q)          # vector bits 9..0
+    CX | c([0, 19])        # control bit 19 (outside any tile), target bit 0
+    steps = plan(lower_circuit(c.gates, n), n, 12, 5)
+    assert len(steps) == 1 and len(steps[0].ops) == len(lower_circuit(c.gates, n))
+
+
+def test_matrix_table_dedups():
+    from quict_b200.simulation.fusion import MatrixTable
+    t = MatrixTable()
+    a = t.add(np.eye(2))
+    b = t.add(np.diag([1, 1j]))
+    c = t.add(np.eye(2))
+    assert a == c and b == 4 and t.size == 8
+
+
+# ---- C-ABI ----------------------------------------------------------------------------
+def _declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "qsim.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(qs_[a-z0-9_]+)\s*\(", txt)))
+
+
+def _lib():
+    from quict_b200 import build
+    from quict_b200 import _native as N
+    if not os.path.exists(N.LIB_PATH):
+        build.build(quiet=True)
+    return N.load()
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib()
+    syms = _declared_symbols()
+    assert len(syms) >= 18
+    for s in syms:
+        assert hasattr(lib, s), s
+    from quict_b200 import _native as N
+    assert set(syms) <= set(N.SIGNATURES), set(syms) - set(N.SIGNATURES)
+
+
+def test_abi_validation_without_gpu():
+    """Bad arguments are rejected on the host before any CUDA call."""
+    lib = _lib()
+    from quict_b200 import _native as N
+    assert lib.qs_version() >= 1
+    m = np.eye(2, dtype=np.complex128)
+    mp = m.ctypes.data_as(C.POINTER(C.c_double))
+    fake = C.c_void_p(0x1000)  # never dereferenced: validation fails first
+    assert lib.qs_apply_1q(None, 4, N.QS_C128, 0, 0, N.QS_K_DENSE, mp, None) == N.QS_EINVAL
+    assert lib.qs_apply_1q(fake, 4, N.QS_C128, 4, 0, N.QS_K_DENSE, mp, None) == N.QS_EINVAL
+    assert b"target bit" in lib.qs_last_error()
+    assert lib.qs_apply_1q(fake, 4, 7, 0, 0, N.QS_K_DENSE, mp, None) == N.QS_EINVAL
+    assert lib.qs_apply_1q(fake, 4, N.QS_C64, 1, 0b10, N.QS_K_DENSE, mp, None) == N.QS_EINVAL
+    assert lib.qs_apply_2q(fake, 4, N.QS_C64, 1, 1, 0, N.QS_K_DENSE, mp, None) == N.QS_EINVAL
+    bits = (C.c_int32 * 3)(0, 1, 1)
+    assert lib.qs_apply_kq(fake, 4, N.QS_C64, 3, bits, 0, fake, None) == N.QS_EINVAL
+    assert lib.qs_prob0(fake, 4, N.QS_C64, N.QS_SRC_SV, 0, None, 0, fake, None) == N.QS_EWORKSPACE
+    assert lib.qs_sample_ws_bytes(20) == 8 * 2 * (1 << 10)
+    # fused: a dense target outside the tile is rejected
+    ps = (N.qs_pass * 1)()
+    ps[0].k, ps[0].nlow, ps[0].op_begin, ps[0].op_count = 3, 2, 0, 1
+    ps[0].hi[0] = 5
+    ops = (N.qs_op * 1)()
+    ops[0].kind, ops[0].m, ops[0].mat = N.QS_OP_MAT, 1, 0
+    ops[0].gbit[0], ops[0].tgt[0] = 4, -1
+    rc = lib.qs_apply_fused(fake, 8, N.QS_C128, ps, 1, ops, 1, fake, 4, None)
+    assert rc == N.QS_EINVAL and b"outside the tile" in lib.qs_last_error()
+    ops[0].gbit[0], ops[0].tgt[0] = 5, 2
+    ops[0].mat = 1  # 4 entries needed from offset 1 in a 4-entry table
+    assert lib.qs_apply_fused(fake, 8, N.QS_C128, ps, 1, ops, 1, fake, 4, None) == N.QS_EINVAL
