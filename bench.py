@@ -219,7 +219,8 @@ def run_ours(args, ws, rank, local):
 
     n = args.qubits
     circuit = config1_circuit(n, N_GATES, SEED)
-    sim = StateVectorSimulator("GPU", "double", gpu_device_id=local, sync=False)
+    sim = StateVectorSimulator("GPU", "double", gpu_device_id=local, sync=False,
+                               max_pass_cost=args.max_pass_cost)
     eng = sim.engine
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -331,6 +332,8 @@ def main():
     ap.add_argument("--ref-gates", type=int, default=24)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-pass-cost", type=float, default=float("inf"),
+                    help="fusion width: per-pass arithmetic bound in dense-1q-gate units")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

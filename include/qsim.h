@@ -58,6 +58,10 @@ extern "C" {
 /* ---- fused-pass op kinds ------------------------------------------------- */
 #define QS_OP_MAT   1     /* dense 2^m x 2^m on m tile-resident bits           */
 #define QS_OP_DIAG  2     /* diagonal on m bits anywhere in the vector         */
+#define QS_OP_ANTI  3     /* m = 1: anti-diagonal 2x2 (entries m01, m10 used)   */
+#define QS_OP_SWAP  4     /* m = 2: swap-like 4x4 (m00, m12, m21, m33 used)     */
+#define QS_MAX_PASS_MATS 2048  /* matrix entries one pass may reference        */
+#define QS_OPF_UNIT 1     /* ANTI: m01 = m10 = 1; SWAP: m00 = m12 = m21 = m33 = 1 */
 
 /* ---- probability sources and sampling modes ------------------------------ */
 #define QS_SRC_SV  0      /* p_i = |vec[i]|^2                                  */
@@ -71,16 +75,16 @@ extern "C" {
 
 /* One op of a fused pass.  64 bytes, plain old data (mirrored by ctypes). */
 typedef struct qs_op {
-    int32_t  kind;       /* QS_OP_MAT or QS_OP_DIAG                             */
+    int32_t  kind;       /* QS_OP_MAT, QS_OP_DIAG, QS_OP_ANTI or QS_OP_SWAP     */
     int32_t  m;          /* number of target bits, 1..4                         */
     int32_t  tgt[4];     /* tile-local position of target j, or -1 when the bit
                             lies outside the tile (allowed for QS_OP_DIAG only) */
     int32_t  gbit[4];    /* vector bit of target j (matrix-index bit m-1-j)     */
     uint32_t lctrl;      /* control mask on tile-local positions                */
-    uint32_t pad0;
+    uint32_t flags;      /* QS_OPF_* hints about the matrix entries             */
     uint64_t gctrl;      /* control mask on vector bits outside the tile        */
     int64_t  mat;        /* element offset of the op's matrix in the table
-                            (QS_OP_MAT: 4^m entries, QS_OP_DIAG: 2^m entries)   */
+                            (QS_OP_DIAG: 2^m entries, the other kinds: 4^m)    */
 } qs_op;
 
 /* One fused pass: a tile of 2^k amplitudes made of vector bits 0..nlow-1 and

@@ -18,7 +18,9 @@ LIB_PATH = os.path.join(_HERE, "libqsim.so")
 QS_OK, QS_EINVAL, QS_ECUDA, QS_EWORKSPACE, QS_ENOTSUP, QS_ETIMEOUT = 0, -1, -2, -3, -4, -5
 QS_C64, QS_C128 = 0, 1
 QS_K_DENSE, QS_K_DIAG, QS_K_ANTIDIAG, QS_K_SWAP = 0, 1, 2, 3
-QS_OP_MAT, QS_OP_DIAG = 1, 2
+QS_OP_MAT, QS_OP_DIAG, QS_OP_ANTI, QS_OP_SWAP = 1, 2, 3, 4
+QS_OPF_UNIT = 1
+QS_MAX_PASS_MATS = 2048
 QS_SRC_SV, QS_SRC_DM = 0, 1
 QS_SAMPLE_CDF, QS_SAMPLE_SEQ = 0, 1
 QS_MAX_TILE_BITS = 14
@@ -44,7 +46,7 @@ class qs_op(C.Structure):
         ("tgt", C.c_int32 * 4),
         ("gbit", C.c_int32 * 4),
         ("lctrl", C.c_uint32),
-        ("pad0", C.c_uint32),
+        ("flags", C.c_uint32),
         ("gctrl", C.c_uint64),
         ("mat", C.c_int64),
     ]

@@ -1,29 +1,81 @@
-// Fused passes: one launch streams the state through shared-memory tiles once
-// and applies every op of the pass to each tile.
+// Fused passes: one launch streams the state through on-chip tiles once and
+// applies every op of the pass to each tile.
 //
 // A tile holds 2^k amplitudes: vector bits 0..nlow-1 (contiguous, so each
-// warp reads 2^nlow consecutive amplitudes) plus k-nlow chosen higher bits.
-// Ops whose non-diagonal targets lie in the tile are applied in shared
-// memory; diagonal factors and controls on bits outside the tile are
-// resolved per tile from the tile's base index, so they fuse into any pass.
+// warp moves 2^nlow consecutive amplitudes) plus k-nlow chosen higher bits.
+// Ops whose non-diagonal targets lie in the tile run on chip; diagonal factors
+// and controls on bits outside the tile are resolved per tile from the tile's
+// base index, so they fuse into any pass.
+//
+// Register-resident kernel (k_fused_reg, tiles of 2^(R+5..R+8)):
+//   each thread owns 2^R amplitudes in registers.  A "layout" assigns R tile
+//   bits to register-slot bits and the remaining tile bits to the thread index
+//   (lanes first).  Ops whose dense targets are slot bits run as fully
+//   unrolled register code (one template per slot mask, no shared memory, no
+//   barriers); between groups of ops ("stages") the tile is re-laid-out
+//   through XOR-swizzled shared memory.  Loads and stores use a layout whose
+//   lanes are tile bits 0..4, i.e. warp-contiguous global runs.  The host
+//   (this file) plans the stages, translates each op into slot / thread /
+//   outside-tile terms and permutes its matrix to the slot order.
+// Shared-memory kernel (k_fused_smem): tiles too small for that layout.
+//
 // The reference has no fusion: one kernel and one full HBM pass per gate
 // (statevector_simulator.py:155-164, gate_function.py:31-1031).
+#include <algorithm>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 
 namespace qs {
 namespace {
 
-constexpr int kFT = 256;  // threads per CTA
+constexpr int kFT = 256;
 
+__host__ __device__ constexpr int popc_c(int x) { return x == 0 ? 0 : (x & 1) + popc_c(x >> 1); }
+// position of the i-th set bit of mask
+__host__ __device__ constexpr int nth_bit(int mask, int i) {
+    int b = 0;
+    while (true) {
+        if ((mask >> b) & 1) {
+            if (i == 0) return b;
+            --i;
+        }
+        ++b;
+    }
+}
+// deposit the low bits of k into the set positions of mask
+__host__ __device__ constexpr int pdep_c(int k, int mask) {
+    int r = 0, i = 0;
+    for (int b = 0; b < 32; ++b)
+        if ((mask >> b) & 1) {
+            if ((k >> i) & 1) r |= 1 << b;
+            ++i;
+        }
+    return r;
+}
+// gather the bits of s at the set positions of mask
+__host__ __device__ constexpr int pext_c(int s, int mask) {
+    int r = 0, i = 0;
+    for (int b = 0; b < 32; ++b)
+        if ((mask >> b) & 1) {
+            if ((s >> b) & 1) r |= 1 << i;
+            ++i;
+        }
+    return r;
+}
+
+__device__ __forceinline__ uint32_t ins0(uint32_t x, int b) {
+    return ((x >> b) << (b + 1)) | (x & ((1u << b) - 1u));
+}
+
+// =============================================================== shared-memory kernel
 struct PassArgs {
     int n, k, nlow, nops;
     int hi[QS_MAX_TILE_BITS];
     qs_op ops[QS_MAX_PASS_OPS];
 };
-
-__device__ __forceinline__ uint32_t ins0(uint32_t x, int b) {
-    return ((x >> b) << (b + 1)) | (x & ((1u << b) - 1u));
-}
 
 template <int M>
 __device__ __forceinline__ void sort_bits(const int* t, int* s) {
@@ -36,7 +88,6 @@ __device__ __forceinline__ void sort_bits(const int* t, int* s) {
             if (s[j] > s[j + 1]) { int x = s[j]; s[j] = s[j + 1]; s[j + 1] = x; }
 }
 
-// Dense 2^M x 2^M on tile-local targets op.tgt[0..M-1].
 template <typename V, int M>
 __device__ __forceinline__ void tile_mat(V* __restrict__ tile, int K, const qs_op& op, const V* __restrict__ mat) {
     constexpr int D = 1 << M;
@@ -55,47 +106,24 @@ __device__ __forceinline__ void tile_mat(V* __restrict__ tile, int K, const qs_o
     }
     const uint32_t lctrl = op.lctrl;
     const uint32_t groups = 1u << (K - M);
-    if (M <= 2) {
-        V mr[D * D];
+    for (uint32_t g = threadIdx.x; g < groups; g += kFT) {
+        uint32_t i0 = g;
 #pragma unroll
-        for (int i = 0; i < D * D; ++i) mr[i] = mat[i];
-        for (uint32_t g = threadIdx.x; g < groups; g += kFT) {
-            uint32_t i0 = g;
+        for (int j = 0; j < M; ++j) i0 = ins0(i0, s[j]);
+        if ((i0 & lctrl) != lctrl) continue;
+        V x[D];
 #pragma unroll
-            for (int j = 0; j < M; ++j) i0 = ins0(i0, s[j]);
-            if ((i0 & lctrl) != lctrl) continue;
-            V x[D];
+        for (int r = 0; r < D; ++r) x[r] = tile[i0 | spread[r]];
 #pragma unroll
-            for (int r = 0; r < D; ++r) x[r] = tile[i0 | spread[r]];
+        for (int r = 0; r < D; ++r) {
+            V acc = cmul(__ldg(&mat[r * D]), x[0]);
 #pragma unroll
-            for (int r = 0; r < D; ++r) {
-                V acc = cmul(mr[r * D], x[0]);
-#pragma unroll
-                for (int c = 1; c < D; ++c) acc = cfma(mr[r * D + c], x[c], acc);
-                tile[i0 | spread[r]] = acc;
-            }
-        }
-    } else {
-        for (uint32_t g = threadIdx.x; g < groups; g += kFT) {
-            uint32_t i0 = g;
-#pragma unroll
-            for (int j = 0; j < M; ++j) i0 = ins0(i0, s[j]);
-            if ((i0 & lctrl) != lctrl) continue;
-            V x[D];
-#pragma unroll
-            for (int r = 0; r < D; ++r) x[r] = tile[i0 | spread[r]];
-#pragma unroll
-            for (int r = 0; r < D; ++r) {
-                V acc = cmul(__ldg(&mat[r * D]), x[0]);
-#pragma unroll
-                for (int c = 1; c < D; ++c) acc = cfma(__ldg(&mat[r * D + c]), x[c], acc);
-                tile[i0 | spread[r]] = acc;
-            }
+            for (int c = 1; c < D; ++c) acc = cfma(__ldg(&mat[r * D + c]), x[c], acc);
+            tile[i0 | spread[r]] = acc;
         }
     }
 }
 
-// Diagonal on op.m bits; bits outside the tile contribute a per-tile constant.
 template <typename V>
 __device__ __forceinline__ void tile_diag(V* __restrict__ tile, int K, uint64_t base, const qs_op& op,
                                           const V* __restrict__ mat) {
@@ -112,33 +140,19 @@ __device__ __forceinline__ void tile_diag(V* __restrict__ tile, int K, uint64_t 
     }
     const uint32_t lctrl = op.lctrl;
     const uint32_t T = 1u << K;
-    if (m <= 2) {
-        V d[4];
+    for (uint32_t e = threadIdx.x; e < T; e += kFT) {
+        if ((e & lctrl) != lctrl) continue;
+        uint32_t sidx = ext;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) d[i] = (i < (1 << m)) ? mat[i] : mk<V>(1.0, 0.0);
-        for (uint32_t e = threadIdx.x; e < T; e += kFT) {
-            if ((e & lctrl) != lctrl) continue;
-            uint32_t sidx = ext;
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-                if (j < m && lpos[j] >= 0) sidx |= ((e >> lpos[j]) & 1u) << (m - 1 - j);
-            tile[e] = cmul(tile[e], d[sidx]);
-        }
-    } else {
-        for (uint32_t e = threadIdx.x; e < T; e += kFT) {
-            if ((e & lctrl) != lctrl) continue;
-            uint32_t sidx = ext;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (j < m && lpos[j] >= 0) sidx |= ((e >> lpos[j]) & 1u) << (m - 1 - j);
-            tile[e] = cmul(tile[e], __ldg(&mat[sidx]));
-        }
+        for (int j = 0; j < 4; ++j)
+            if (j < m && lpos[j] >= 0) sidx |= ((e >> lpos[j]) & 1u) << (m - 1 - j);
+        tile[e] = cmul(tile[e], __ldg(&mat[sidx]));
     }
 }
 
 template <typename V>
-__global__ void __launch_bounds__(kFT) k_fused(V* __restrict__ vec, const __grid_constant__ PassArgs p,
-                                                const V* __restrict__ mats) {
+__global__ void __launch_bounds__(kFT) k_fused_smem(V* __restrict__ vec, const __grid_constant__ PassArgs p,
+                                                     const V* __restrict__ mats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = p.k, L = p.nlow, H = K - L;
     const uint32_t T = 1u << K;
@@ -156,31 +170,455 @@ __global__ void __launch_bounds__(kFT) k_fused(V* __restrict__ vec, const __grid
     for (uint64_t tid = blockIdx.x; tid < ntiles; tid += gridDim.x) {
         uint64_t base = tid << L;
         for (int t = 0; t < H; ++t) base = insert0(base, p.hi[t]);
-        for (uint32_t e = threadIdx.x; e < T; e += kFT)
-            tile[e] = vec[base | hoff[e >> L] | (e & lmask)];
+        for (uint32_t e = threadIdx.x; e < T; e += kFT) tile[e] = vec[base | hoff[e >> L] | (e & lmask)];
         __syncthreads();
         for (int o = 0; o < p.nops; ++o) {
             const qs_op& op = p.ops[o];
             if ((base & op.gctrl) != op.gctrl) continue;  // CTA-uniform
             const V* mat = mats + op.mat;
-            if (op.kind == QS_OP_MAT) {
+            if (op.kind == QS_OP_DIAG) {
+                tile_diag<V>(tile, K, base, op, mat);
+            } else {
                 switch (op.m) {
                     case 1: tile_mat<V, 1>(tile, K, op, mat); break;
                     case 2: tile_mat<V, 2>(tile, K, op, mat); break;
                     case 3: tile_mat<V, 3>(tile, K, op, mat); break;
                     default: tile_mat<V, 4>(tile, K, op, mat); break;
                 }
-            } else {
-                tile_diag<V>(tile, K, base, op, mat);
             }
             __syncthreads();
         }
-        for (uint32_t e = threadIdx.x; e < T; e += kFT)
-            vec[base | hoff[e >> L] | (e & lmask)] = tile[e];
+        for (uint32_t e = threadIdx.x; e < T; e += kFT) vec[base | hoff[e >> L] | (e & lmask)] = tile[e];
         __syncthreads();
     }
 }
 
+// ============================================================ register-resident kernel
+constexpr int kMaxStages = 40;
+
+struct KOp {
+    uint8_t code;     // QS_OP_MAT / DIAG / ANTI / SWAP
+    uint8_t mask;     // slot-bit mask of the targets held in registers
+    uint8_t scm;      // control mask on slot bits
+    uint8_t nh;       // DIAG: targets outside the registers
+    uint8_t hsrc[4];  // DIAG: their sources: < 64 tile bit, >= 64 vector bit + 64
+    uint16_t tctrl;   // control mask on the thread's tile bits
+    uint16_t moff;    // shared-memory offset of the slot-ordered matrix
+    uint8_t flags;
+    uint8_t pad[3];
+    uint64_t gctrl;   // control mask on vector bits outside the tile
+};
+struct KCopy {
+    int64_t goff;     // table offset of the stored matrix
+    uint16_t soff;    // shared-memory offset
+    uint8_t m;
+    uint8_t diag;
+    uint8_t perm[4];  // slot-order index bit i -> stored index bit perm[i]
+};
+struct KStage {
+    uint8_t R[6];     // slot bit j <-> tile bit R[j]
+    uint8_t T[8];     // thread bit i <-> tile bit T[i]
+    uint16_t op_begin, op_count;
+};
+struct RegArgs {
+    int n, K, L, H, nT, nstages, nops, nmats;
+    int hi[QS_MAX_TILE_BITS];
+    KStage st[kMaxStages];
+    KOp ops[QS_MAX_PASS_OPS];
+    KCopy cp[QS_MAX_PASS_OPS];
+};
+
+template <typename V>
+__device__ __forceinline__ uint32_t swz(uint32_t t) {
+    if (sizeof(V) == 16) return t ^ (((t >> 3) ^ (t >> 6) ^ (t >> 9) ^ (t >> 12)) & 7u);
+    return t ^ (((t >> 4) ^ (t >> 8) ^ (t >> 12)) & 15u);
+}
+
+__device__ __forceinline__ bool ctrl_ok(int s, uint32_t scm) { return (uint32_t(s) & scm) == scm; }
+
+// compile-time loop: f(std::integral_constant<int, i>) for i in [0, N)
+template <typename F, int... I>
+__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+    sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// Buffer address of slot s for the current stage: tpos ^ XOR_{j in s} rpos[j].
+// (The swizzle is linear over GF(2), so a swizzled address splits the same way.)
+template <int R>
+struct Addr {
+    uint32_t tpos;
+    uint32_t rpos[R];
+    template <int S>
+    __device__ __forceinline__ uint32_t at() const {
+        uint32_t t = tpos;
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+            if ((S >> j) & 1) t ^= rpos[j];
+        return t;
+    }
+};
+
+// ---- dense op on the slot bits of MASK (slot-order matrix in shared memory).
+// Small matrices keep inputs and outputs in registers; for 8x8 / 16x16 each
+// output row goes to this thread's own positions of the tile buffer and is read
+// back after the group.  No other thread reads or writes those positions: the
+// thread holds exactly the amplitudes stored there (plain order in the first
+// stage, swizzled order after a relayout; `ad` addresses whichever applies).
+// PRED: some of the op's controls are slot bits (checked per group).
+template <typename V, int E, int R, int MASK, bool PRED>
+__device__ __forceinline__ void r_mat(V (&x)[E], const V* __restrict__ Mm, uint32_t scm, V* __restrict__ buf,
+                                      const Addr<R>& ad) {
+    constexpr int M = popc_c(MASK);
+    constexpr int D = 1 << M;
+    constexpr bool PRELOAD = sizeof(V) == 16 ? (M == 1) : (M <= 2);
+    constexpr bool BIG = M >= 3;
+    V mr[PRELOAD ? D * D : 1];
+    if constexpr (PRELOAD) {
+#pragma unroll
+        for (int i = 0; i < D * D; ++i) mr[i] = Mm[i];
+    }
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        if constexpr ((s & MASK) == 0) {
+            if (!PRED || ctrl_ok(s, scm)) {
+                if constexpr (BIG) {
+                    sfor<D>([&](auto rc) __attribute__((always_inline)) {
+                        constexpr int r = decltype(rc)::value;
+                        V acc = cmul(Mm[r * D], x[s]);
+                        sfor<D - 1>([&](auto cc) __attribute__((always_inline)) {
+                            constexpr int c = decltype(cc)::value + 1;
+                            acc = cfma(Mm[r * D + c], x[s | pdep_c(c, MASK)], acc);
+                        });
+                        buf[ad.template at<(s | pdep_c(r, MASK))>()] = acc;
+                    });
+                    sfor<D>([&](auto rc) __attribute__((always_inline)) {
+                        constexpr int o = s | pdep_c(decltype(rc)::value, MASK);
+                        x[o] = buf[ad.template at<o>()];
+                    });
+                } else {
+                    V xi[D];
+                    sfor<D>([&](auto kc) __attribute__((always_inline)) {
+                        constexpr int k = decltype(kc)::value;
+                        xi[k] = x[s | pdep_c(k, MASK)];
+                    });
+                    sfor<D>([&](auto rc) __attribute__((always_inline)) {
+                        constexpr int r = decltype(rc)::value;
+                        V acc = cmul(PRELOAD ? mr[PRELOAD ? r * D : 0] : Mm[r * D], xi[0]);
+#pragma unroll
+                        for (int c = 1; c < D; ++c)
+                            acc = cfma(PRELOAD ? mr[PRELOAD ? r * D + c : 0] : Mm[r * D + c], xi[c], acc);
+                        x[s | pdep_c(r, MASK)] = acc;
+                    });
+                }
+            }
+        }
+    });
+}
+
+// ---- anti-diagonal 2x2 on one slot bit (UNIT: plain exchange)
+template <typename V, int E, int MASK, bool PRED, bool UNIT>
+__device__ __forceinline__ void r_anti(V (&x)[E], const V* __restrict__ Mm, uint32_t scm) {
+    V m01, m10;
+    if constexpr (!UNIT) {
+        m01 = Mm[1];
+        m10 = Mm[2];
+    }
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        if constexpr ((s & MASK) == 0) {
+            if (!PRED || ctrl_ok(s, scm)) {
+                V a = x[s];
+                if constexpr (UNIT) {
+                    x[s] = x[s | MASK];
+                    x[s | MASK] = a;
+                } else {
+                    x[s] = cmul(m01, x[s | MASK]);
+                    x[s | MASK] = cmul(m10, a);
+                }
+            }
+        }
+    });
+}
+
+// ---- swap-like 4x4 on two slot bits (slot order: index 1 = lower bit)
+template <typename V, int E, int MASK, bool PRED, bool UNIT>
+__device__ __forceinline__ void r_swap(V (&x)[E], const V* __restrict__ Mm, uint32_t scm) {
+    constexpr int B0 = 1 << nth_bit(MASK, 0), B1 = 1 << nth_bit(MASK, 1);
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        if constexpr ((s & MASK) == 0) {
+            if (!PRED || ctrl_ok(s, scm)) {
+                V a = x[s | B0];
+                if constexpr (UNIT) {
+                    x[s | B0] = x[s | B1];
+                    x[s | B1] = a;
+                } else {
+                    x[s | B0] = cmul(Mm[6], x[s | B1]);
+                    x[s | B1] = cmul(Mm[9], a);
+                    x[s] = cmul(Mm[0], x[s]);
+                    x[s | B0 | B1] = cmul(Mm[15], x[s | B0 | B1]);
+                }
+            }
+        }
+    });
+}
+
+// ---- diagonal: index = (outside-register bits) << popc(SM) | slot bits of SM
+template <typename V, int E, int SM, bool PRED>
+__device__ __forceinline__ void r_diag(V (&x)[E], const V* __restrict__ Dm, uint32_t scm, uint32_t h) {
+    constexpr int NS = popc_c(SM);
+    const V* d = Dm + (h << NS);
+    constexpr bool PRELOAD = NS <= 2;
+    V dv[PRELOAD ? (1 << NS) : 1];
+    if constexpr (PRELOAD) {
+#pragma unroll
+        for (int i = 0; i < (1 << NS); ++i) dv[i] = d[i];
+    }
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        constexpr int k = pext_c(s, SM);
+        if (!PRED || ctrl_ok(s, scm)) x[s] = cmul(x[s], PRELOAD ? dv[PRELOAD ? k : 0] : d[k]);
+    });
+}
+
+#define QS_MASKS_1_31(F)                                                                             \
+    F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15) F(16) F(17) \
+        F(18) F(19) F(20) F(21) F(22) F(23) F(24) F(25) F(26) F(27) F(28) F(29) F(30) F(31)
+
+template <typename V, int R>
+__device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* __restrict__ msm, uint32_t thr,
+                                        uint64_t base, V* __restrict__ buf, const Addr<R>& ad) {
+    constexpr int E = 1 << R;
+    const V* Mm = msm + op.moff;
+    const uint32_t scm = op.scm;
+    const bool pred = scm != 0;
+    const bool unit = op.flags & QS_OPF_UNIT;
+    switch (op.code) {
+        case QS_OP_MAT:
+            switch (op.mask) {
+#define QS_CASE(MK)                                                                  \
+    case MK:                                                                         \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) <= 2) {                          \
+            if (pred) r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                 \
+            else r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                     \
+        } else if constexpr ((MK) < (1 << R) && popc_c(MK) <= 4) {                   \
+            r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                           \
+        }                                                                            \
+        break;
+                QS_MASKS_1_31(QS_CASE)
+#undef QS_CASE
+            }
+            break;
+        case QS_OP_ANTI:
+            switch (op.mask) {
+#define QS_CASE(MK)                                                                  \
+    case MK:                                                                         \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) == 1) {                          \
+            if (unit) {                                                              \
+                if (pred) r_anti<V, E, MK, true, true>(x, Mm, scm);                  \
+                else r_anti<V, E, MK, false, true>(x, Mm, scm);                      \
+            } else {                                                                 \
+                if (pred) r_anti<V, E, MK, true, false>(x, Mm, scm);                 \
+                else r_anti<V, E, MK, false, false>(x, Mm, scm);                     \
+            }                                                                        \
+        }                                                                            \
+        break;
+                QS_MASKS_1_31(QS_CASE)
+#undef QS_CASE
+            }
+            break;
+        case QS_OP_SWAP:
+            switch (op.mask) {
+#define QS_CASE(MK)                                                                  \
+    case MK:                                                                         \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) == 2) {                          \
+            if (unit) r_swap<V, E, MK, true, true>(x, Mm, scm);                      \
+            else r_swap<V, E, MK, true, false>(x, Mm, scm);                          \
+        }                                                                            \
+        break;
+                QS_MASKS_1_31(QS_CASE)
+#undef QS_CASE
+            }
+            break;
+        default: {  // QS_OP_DIAG
+            uint32_t h = 0;
+            for (int q = 0; q < op.nh; ++q) {
+                const int src = op.hsrc[q];
+                const uint32_t bit = src < 64 ? (thr >> src) & 1u : uint32_t((base >> (src - 64)) & 1u);
+                h = (h << 1) | bit;
+            }
+            switch (op.mask) {
+                case 0:
+                    if (pred) r_diag<V, E, 0, true>(x, Mm, scm, h);
+                    else r_diag<V, E, 0, false>(x, Mm, scm, h);
+                    break;
+#define QS_CASE(MK)                                                                  \
+    case MK:                                                                         \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) <= 4) {                          \
+            if (pred) r_diag<V, E, MK, true>(x, Mm, scm, h);                         \
+            else r_diag<V, E, MK, false>(x, Mm, scm, h);                             \
+        }                                                                            \
+        break;
+                QS_MASKS_1_31(QS_CASE)
+#undef QS_CASE
+            }
+        }
+    }
+}
+
+// thread part (tile bits) of a stage layout
+template <int R>
+__device__ __forceinline__ uint32_t thread_bits(const KStage& S, int nT) {
+    uint32_t t = 0;
+    for (int i = 0; i < nT; ++i)
+        if ((threadIdx.x >> i) & 1) t |= 1u << S.T[i];
+    return t;
+}
+
+template <typename V, int R>
+__device__ __forceinline__ Addr<R> stage_addr(const KStage& S, int nT, bool swizzled) {
+    Addr<R> a;
+    const uint32_t t = thread_bits<R>(S, nT);
+    a.tpos = swizzled ? swz<V>(t) : t;
+#pragma unroll
+    for (int j = 0; j < R; ++j) a.rpos[j] = swizzled ? swz<V>(1u << S.R[j]) : (1u << S.R[j]);
+    return a;
+}
+
+// Re-layout the registers from the current addressing `from` into stage B's
+// (swizzled) addressing; returns B's addressing.
+template <typename V, int R>
+__device__ __forceinline__ Addr<R> r_relayout(V (&x)[1 << R], V* __restrict__ buf, const KStage& A, const KStage& B,
+                                              int nT) {
+    constexpr int E = 1 << R;
+    const Addr<R> aw = stage_addr<V, R>(A, nT, true);
+    const Addr<R> ar = stage_addr<V, R>(B, nT, true);
+    __syncthreads();  // previous readers of buf are done
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        buf[aw.template at<s>()] = x[s];
+    });
+    __syncthreads();
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        x[s] = buf[ar.template at<s>()];
+    });
+    return ar;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Copy one tile (2^K amplitudes) into `dst` in plain tile order with 16-byte
+// cp.async chunks (one chunk = 16 / sizeof(V) consecutive amplitudes).
+template <typename V>
+__device__ __forceinline__ void tile_prefetch(V* __restrict__ dst, const V* __restrict__ vec, uint64_t base, int K,
+                                              int L, const uint64_t* __restrict__ hoff) {
+    constexpr int EPC = 16 / sizeof(V);
+    const uint32_t chunks = (1u << K) / EPC;
+    const uint32_t lmask = (1u << L) - 1u;
+    for (uint32_t c = threadIdx.x; c < chunks; c += blockDim.x) {
+        const uint32_t e = c * EPC;
+        cp_async16(dst + e, vec + (base | hoff[e >> L] | (e & lmask)));
+    }
+    cp_async_commit();
+}
+
+template <typename V, int R>
+__global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const __grid_constant__ RegArgs p,
+                                                      const V* __restrict__ mats) {
+    constexpr int E = 1 << R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = p.K, L = p.L, H = p.H, nT = p.nT;
+    V* bufs[2] = {reinterpret_cast<V*>(smem_raw), reinterpret_cast<V*>(smem_raw) + (size_t(1) << K)};
+    V* msm = bufs[1] + (size_t(1) << K);
+    uint64_t* hoff = reinterpret_cast<uint64_t*>(msm + p.nmats);
+    uint64_t* gslot_store = hoff + (size_t(1) << H);  // E entries: global offset of each slot
+    // stage the pass's matrices in slot order; tile high-bit offsets
+    for (int o = 0; o < p.nops; ++o) {
+        const KCopy& c = p.cp[o];
+        const int D = 1 << c.m;
+        const int cnt = c.diag ? D : D * D;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
+            int sr = 0, sc = 0;
+            for (int i = 0; i < c.m; ++i) {
+                sr |= ((kr >> i) & 1) << c.perm[i];
+                sc |= ((kc >> i) & 1) << c.perm[i];
+            }
+            msm[c.soff + e] = mats[c.goff + (c.diag ? sr : sr * D + sc)];
+        }
+    }
+    for (uint32_t j = threadIdx.x; j < (1u << H); j += blockDim.x) {
+        uint64_t o = 0;
+        for (int t = 0; t < H; ++t)
+            if ((j >> t) & 1) o |= uint64_t(1) << p.hi[t];
+        hoff[j] = o;
+    }
+    auto gbit = [&](int b) -> uint64_t { return uint64_t(1) << (b < L ? b : p.hi[b - L]); };
+    const KStage& SL = p.st[p.nstages - 1];
+    for (int s2 = threadIdx.x; s2 < E; s2 += blockDim.x) {
+        uint64_t o = 0;
+        for (int j = 0; j < R; ++j)
+            if ((s2 >> j) & 1) o |= gbit(SL.R[j]);
+        gslot_store[s2] = o;
+    }
+    uint64_t gthr_store = 0;
+    for (int i = 0; i < nT; ++i)
+        if ((threadIdx.x >> i) & 1) gthr_store |= gbit(SL.T[i]);
+    __syncthreads();
+    const uint64_t ntiles = uint64_t(1) << (p.n - K);
+    auto tile_base = [&](uint64_t tile) {
+        uint64_t b = tile << L;
+        for (int t = 0; t < H; ++t) b = insert0(b, p.hi[t]);
+        return b;
+    };
+    uint64_t tile = blockIdx.x;
+    if (tile < ntiles) tile_prefetch<V>(bufs[0], vec, tile_base(tile), K, L, hoff);
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        V* cur = bufs[it & 1];
+        const uint64_t base = tile_base(tile);
+        cp_async_wait_all();
+        __syncthreads();  // tile landed; the other buffer is free
+        if (tile + gridDim.x < ntiles) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + gridDim.x), K, L, hoff);
+        V x[E];
+        // shared memory -> registers in the first stage's (plain) layout
+        Addr<R> ad = stage_addr<V, R>(p.st[0], nT, false);
+        sfor<E>([&](auto sc) __attribute__((always_inline)) {
+            constexpr int s = decltype(sc)::value;
+            x[s] = cur[ad.template at<s>()];
+        });
+        for (int si = 0; si < p.nstages; ++si) {
+            const KStage& S = p.st[si];
+            if (si > 0) ad = r_relayout<V, R>(x, cur, p.st[si - 1], S, nT);
+            const uint32_t thr = thread_bits<R>(S, nT);
+            const int oe = S.op_begin + S.op_count;
+            for (int o = S.op_begin; o < oe; ++o) {
+                const KOp& op = p.ops[o];
+                if ((base & op.gctrl) != op.gctrl) continue;
+                if ((thr & op.tctrl) != op.tctrl) continue;
+                r_apply<V, R>(x, op, msm, thr, base, cur, ad);
+            }
+        }
+        {  // registers -> global in the last stage's layout (lanes on tile bits 0..4)
+            const uint64_t b0 = base | gthr_store;
+            sfor<E>([&](auto sc) __attribute__((always_inline)) {
+                constexpr int s = decltype(sc)::value;
+                vec[b0 | gslot_store[s]] = x[s];
+            });
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host side
 int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total, int64_t mats_count) {
     QS_REQUIRE(ps.k >= 1 && ps.k <= QS_MAX_TILE_BITS && ps.k <= n, "tile bits %d outside [1, min(%d, n)]", ps.k,
                QS_MAX_TILE_BITS);
@@ -195,56 +633,240 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
         prev = ps.hi[t];
         tilemask |= uint64_t(1) << ps.hi[t];
     }
-    // global bit -> local position
     int local[64];
     for (int b = 0; b < 64; ++b) local[b] = -1;
     for (int b = 0; b < ps.nlow; ++b) local[b] = b;
     for (int t = 0; t < ps.k - ps.nlow; ++t) local[ps.hi[t]] = ps.nlow + t;
     for (int i = 0; i < ps.op_count; ++i) {
         const qs_op& op = ops[ps.op_begin + i];
-        QS_REQUIRE(op.kind == QS_OP_MAT || op.kind == QS_OP_DIAG, "op %d: bad kind %d", i, op.kind);
+        QS_REQUIRE(op.kind >= QS_OP_MAT && op.kind <= QS_OP_SWAP, "op %d: bad kind %d", i, op.kind);
         QS_REQUIRE(op.m >= 1 && op.m <= 4, "op %d: m=%d outside [1, 4]", i, op.m);
+        QS_REQUIRE(op.kind != QS_OP_ANTI || op.m == 1, "op %d: ANTI needs m = 1", i);
+        QS_REQUIRE(op.kind != QS_OP_SWAP || op.m == 2, "op %d: SWAP needs m = 2", i);
         QS_REQUIRE((op.gctrl >> n) == 0 && (op.gctrl & tilemask) == 0, "op %d: global controls must lie outside the tile", i);
         QS_REQUIRE((op.lctrl >> ps.k) == 0, "op %d: local controls outside the tile", i);
         uint32_t tl = 0;
         for (int j = 0; j < op.m; ++j) {
             QS_REQUIRE(op.gbit[j] >= 0 && op.gbit[j] < n, "op %d: target bit outside [0, n)", i);
             QS_REQUIRE(op.tgt[j] == local[op.gbit[j]], "op %d: tile position of target %d inconsistent", i, j);
-            if (op.kind == QS_OP_MAT) QS_REQUIRE(op.tgt[j] >= 0, "op %d: dense target outside the tile", i);
+            if (op.kind != QS_OP_DIAG) QS_REQUIRE(op.tgt[j] >= 0, "op %d: dense target outside the tile", i);
             if (op.tgt[j] >= 0) {
                 QS_REQUIRE(!((tl >> op.tgt[j]) & 1), "op %d: duplicate target", i);
                 tl |= 1u << op.tgt[j];
             }
         }
         QS_REQUIRE((tl & op.lctrl) == 0, "op %d: control overlaps a target", i);
-        int64_t len = op.kind == QS_OP_MAT ? (int64_t(1) << (2 * op.m)) : (int64_t(1) << op.m);
+        int64_t len = op.kind == QS_OP_DIAG ? (int64_t(1) << op.m) : (int64_t(1) << (2 * op.m));
         QS_REQUIRE(op.mat >= 0 && op.mat + len <= mats_count, "op %d: matrix outside the table", i);
     }
     return QS_OK;
 }
 
 template <typename V>
-int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
-    static thread_local PassArgs args;  // ~10 KB, keep off the stack
+void config_smem(const void* fn) {
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        done[dev] = 1;
+    }
+}
+
+template <typename V>
+int launch_smem(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+    static thread_local PassArgs args;
     args.n = n; args.k = ps.k; args.nlow = ps.nlow; args.nops = ps.op_count;
     for (int t = 0; t < QS_MAX_TILE_BITS; ++t) args.hi[t] = t < ps.k - ps.nlow ? ps.hi[t] : 0;
     for (int i = 0; i < ps.op_count; ++i) args.ops[i] = ops[ps.op_begin + i];
     size_t smem = sizeof(V) * (size_t(1) << ps.k) + sizeof(uint64_t) * (size_t(1) << (ps.k - ps.nlow));
-    static int configured[2] = {0, 0};
-    int slot = sizeof(V) == 16 ? 1 : 0;
-    if (!configured[slot]) {
-        cudaFuncSetAttribute(k_fused<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured[slot] = 1;
-    }
+    config_smem<V>((const void*)k_fused_smem<V>);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<V>, kFT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_smem<V>, kFT, smem);
     if (occ < 1) occ = 1;
     uint64_t ntiles = uint64_t(1) << (n - ps.k);
     uint64_t cap = uint64_t(sm_count()) * occ;
-    unsigned grid = unsigned(ntiles < cap ? ntiles : cap);
-    k_fused<V><<<grid, kFT, smem, st>>>(vec, args, mats);
-    QS_CHECK_LAUNCH("qs_apply_fused");
+    k_fused_smem<V><<<unsigned(ntiles < cap ? ntiles : cap), kFT, smem, st>>>(vec, args, mats);
+    QS_CHECK_LAUNCH("qs_apply_fused(smem)");
     return QS_OK;
+}
+
+// Build the register-kernel arguments for ops [first, ...) of a pass; returns
+// the number of ops consumed (a pass whose stages or matrices overflow the
+// argument block is split into several launches over the same tile).
+int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegArgs& a) {
+    const int K = ps.k, L = ps.nlow, nT = K - R;
+    a.n = n; a.K = K; a.L = L; a.H = K - L; a.nT = nT;
+    for (int t = 0; t < QS_MAX_TILE_BITS; ++t) a.hi[t] = t < K - L ? ps.hi[t] : 0;
+    const int lowlanes = 5;  // tile bits 0..4 are the lanes of the load/store layout
+    auto xbits = [&](const qs_op& op) {
+        std::vector<int> v;
+        if (op.kind != QS_OP_DIAG)
+            for (int j = 0; j < op.m; ++j) v.push_back(op.tgt[j]);
+        return v;
+    };
+    auto make_stage = [&](const std::vector<int>& regs, KStage& S) {
+        for (int j = 0; j < 6; ++j) S.R[j] = j < R ? uint8_t(regs[j]) : 0;
+        int i = 0;
+        for (int b = 0; b < K; ++b)
+            if (std::find(regs.begin(), regs.end(), b) == regs.end()) S.T[i++] = uint8_t(b);
+        for (; i < 8; ++i) S.T[i] = 0;
+    };
+    const int count = ps.op_count - first;
+    // initial (load) layout: register bits among tile bits >= 5, preferring early targets
+    std::vector<int> cur;
+    for (int i = 0; i < count && int(cur.size()) < R; ++i)
+        for (int b : xbits(ops[ps.op_begin + first + i]))
+            if (b >= lowlanes && int(cur.size()) < R && std::find(cur.begin(), cur.end(), b) == cur.end())
+                cur.push_back(b);
+    for (int b = K - 1; b >= lowlanes && int(cur.size()) < R; --b)
+        if (std::find(cur.begin(), cur.end(), b) == cur.end()) cur.push_back(b);
+    const std::vector<int> load_layout = cur;
+    int ns = 0, nops = 0, moff = 0;
+    make_stage(cur, a.st[0]);
+    a.st[0].op_begin = 0;
+    a.st[0].op_count = 0;
+    ns = 1;
+    int consumed = 0;
+    for (int i = 0; i < count; ++i) {
+        const qs_op& op = ops[ps.op_begin + first + i];
+        const int msize = op.kind == QS_OP_DIAG ? (1 << op.m) : (1 << (2 * op.m));
+        if (moff + msize > QS_MAX_PASS_MATS) break;
+        std::vector<int> xb = xbits(op);
+        bool fits = true;
+        for (int b : xb)
+            if (std::find(cur.begin(), cur.end(), b) == cur.end()) fits = false;
+        if (!fits) {
+            if (ns + 2 > kMaxStages) break;  // keep room for a final store layout
+            std::vector<int> nx = xb;
+            for (int k2 = i + 1; k2 < count; ++k2) {
+                std::vector<int> xb2 = xbits(ops[ps.op_begin + first + k2]);
+                std::vector<int> u = nx;
+                for (int b : xb2)
+                    if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
+                if (int(u.size()) > R) break;
+                nx = u;
+            }
+            for (int b : cur)
+                if (int(nx.size()) < R && std::find(nx.begin(), nx.end(), b) == nx.end()) nx.push_back(b);
+            for (int b = K - 1; b >= 0 && int(nx.size()) < R; --b)
+                if (std::find(nx.begin(), nx.end(), b) == nx.end()) nx.push_back(b);
+            cur = nx;
+            make_stage(cur, a.st[ns]);
+            a.st[ns].op_begin = uint16_t(nops);
+            a.st[ns].op_count = 0;
+            ++ns;
+        }
+        // translate the op into the current layout
+        KStage& S = a.st[ns - 1];
+        auto slot_of = [&](int b) {
+            for (int j = 0; j < R; ++j)
+                if (S.R[j] == b) return j;
+            return -1;
+        };
+        KOp& k = a.ops[nops];
+        KCopy& c = a.cp[nops];
+        k = KOp{};
+        c = KCopy{};
+        k.code = uint8_t(op.kind);
+        k.flags = uint8_t(op.flags);
+        k.gctrl = op.gctrl;
+        uint32_t scm = 0, tct = 0;
+        for (int b = 0; b < K; ++b)
+            if ((op.lctrl >> b) & 1) {
+                int sl = slot_of(b);
+                if (sl >= 0) scm |= 1u << sl;
+                else tct |= 1u << b;
+            }
+        k.scm = uint8_t(scm);
+        k.tctrl = uint16_t(tct);
+        c.goff = op.mat;
+        c.soff = uint16_t(moff);
+        c.m = uint8_t(op.m);
+        c.diag = op.kind == QS_OP_DIAG;
+        k.moff = uint16_t(moff);
+        // slot-ordered bit permutation
+        int slots[4], js[4], ns_ = 0;
+        int hj[4], nh = 0;
+        for (int j = 0; j < op.m; ++j) {
+            int sl = op.tgt[j] >= 0 ? slot_of(op.tgt[j]) : -1;
+            if (sl >= 0) {
+                slots[ns_] = sl;
+                js[ns_++] = j;
+            } else {
+                hj[nh++] = j;
+            }
+        }
+        for (int x = 0; x < ns_; ++x)  // sort by slot position
+            for (int y = 0; y + 1 < ns_ - x; ++y)
+                if (slots[y] > slots[y + 1]) {
+                    std::swap(slots[y], slots[y + 1]);
+                    std::swap(js[y], js[y + 1]);
+                }
+        uint32_t mask = 0;
+        for (int x = 0; x < ns_; ++x) {
+            mask |= 1u << slots[x];
+            c.perm[x] = uint8_t(op.m - 1 - js[x]);
+        }
+        for (int q = 0; q < nh; ++q) {
+            c.perm[ns_ + (nh - 1 - q)] = uint8_t(op.m - 1 - hj[q]);
+            const int j = hj[q];
+            k.hsrc[q] = op.tgt[j] >= 0 ? uint8_t(op.tgt[j]) : uint8_t(64 + op.gbit[j]);
+        }
+        k.mask = uint8_t(mask);
+        k.nh = uint8_t(nh);
+        moff += msize;
+        ++nops;
+        ++S.op_count;
+        ++consumed;
+    }
+    // final store layout must keep the lanes on tile bits 0..4
+    bool low_in_regs = false;
+    for (int b : cur)
+        if (b < lowlanes) low_in_regs = true;
+    if (low_in_regs) {
+        make_stage(load_layout, a.st[ns]);
+        a.st[ns].op_begin = uint16_t(nops);
+        a.st[ns].op_count = 0;
+        ++ns;
+    }
+    a.nstages = ns;
+    a.nops = nops;
+    a.nmats = moff;
+    return consumed;
+}
+
+template <typename V, int R>
+int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+    static thread_local RegArgs args;
+    config_smem<V>((const void*)k_fused_reg<V, R>);
+    int first = 0;
+    while (first < ps.op_count) {
+        int used = build_reg(ps, ops, first, n, R, args);
+        if (used <= 0) {
+            set_error("qs_apply_fused: op %d does not fit a register tile", ps.op_begin + first);
+            return QS_EINVAL;
+        }
+        size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R));
+        uint64_t ntiles = uint64_t(1) << (n - ps.k);
+        uint64_t cap = uint64_t(sm_count());
+        k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), 1 << (ps.k - R), smem, st>>>(vec, args, mats);
+        QS_CHECK_LAUNCH("qs_apply_fused(reg)");
+        first += used;
+    }
+    return QS_OK;
+}
+
+template <typename V>
+constexpr int reg_bits() { return sizeof(V) == 16 ? 4 : 5; }
+
+template <typename V>
+int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+    constexpr int R = reg_bits<V>();
+    const int nT = ps.k - R;
+    const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R));
+    if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
+    return launch_smem<V>(vec, n, ps, ops, mats, st);
 }
 
 }  // namespace
@@ -265,7 +887,7 @@ extern "C" int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes
         int rc = validate_pass(passes[i], n, ops, nops_total, mats_count);
         if (rc) return rc;
         size_t smem = vsize * (size_t(1) << passes[i].k) + 8 * (size_t(1) << (passes[i].k - passes[i].nlow));
-        QS_REQUIRE(smem <= 200 * 1024, "pass %d: tile of 2^%d needs %zu bytes of shared memory", i, passes[i].k, smem);
+        QS_REQUIRE(smem <= 160 * 1024, "pass %d: tile of 2^%d needs %zu bytes of shared memory", i, passes[i].k, smem);
     }
     for (int i = 0; i < npasses; ++i) {
         if (passes[i].op_count == 0) continue;

@@ -84,6 +84,7 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
         xblk: set = set()
         zblk: set = set()
         cost = 0.0
+        entries = 0
         stop = False
         for idx, op in enumerate(pending):
             if stop:
@@ -99,11 +100,13 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
             hoistable = not (allb & xblk) and not (xb & zblk)
             need = xb - low - hi
             c = op_cost(op)
+            ent = op_entries(op)
             if (hoistable and len(hi) + len(need) <= H and len(chosen) < max_ops
-                    and (cost + c <= max_cost or not chosen)):
+                    and entries + ent <= N.QS_MAX_PASS_MATS and (cost + c <= max_cost or not chosen)):
                 hi |= need
                 chosen.append(op)
                 cost += c
+                entries += ent
             else:
                 deferred.append(op)
                 xblk |= xb
@@ -117,6 +120,11 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
         steps.append(Pass(k, nlow, tuple(sorted(hi)), chosen))
         pending = deferred
     return steps
+
+
+def op_entries(op: Op) -> int:
+    """Matrix entries the op occupies in a pass's on-chip matrix table."""
+    return (1 << op.m) if op.kind == "diag" else (1 << (2 * op.m))
 
 
 def op_cost(op: Op) -> float:
@@ -187,10 +195,16 @@ def emit(passes: Sequence[Pass], table: MatrixTable):
                 else:
                     gc |= 1 << b
             c.lctrl, c.gctrl = lc, gc
+            c.flags = 0
             if op.kind == "diag":
                 c.kind = N.QS_OP_DIAG
                 c.mat = table.add(op.mat)
             else:
-                c.kind = N.QS_OP_MAT
+                c.kind = {"mat": N.QS_OP_MAT, "antidiag": N.QS_OP_ANTI, "swap": N.QS_OP_SWAP}[op.kind]
                 c.mat = table.add(op.dense())
+                if op.kind == "antidiag" and op.mat[0, 1] == 1 and op.mat[1, 0] == 1:
+                    c.flags = N.QS_OPF_UNIT
+                if (op.kind == "swap" and op.mat[0, 0] == 1 and op.mat[1, 2] == 1 and op.mat[2, 1] == 1
+                        and op.mat[3, 3] == 1):
+                    c.flags = N.QS_OPF_UNIT
     return cps, len(passes), cops, nops

@@ -97,8 +97,8 @@ def _every_placement_circuit(n, seed):
     return gl
 
 
-@pytest.mark.parametrize("n", [6, 9, 14])
-@pytest.mark.parametrize("tile", [(None, None), (8, 3), (6, 0), (10, 5)])
+@pytest.mark.parametrize("n", [6, 9, 14, 17])
+@pytest.mark.parametrize("tile", [(None, None), (8, 3), (6, 0), (10, 5), (11, 5)])
 def test_every_gate_every_placement_vs_oracle(cuda_ok, n, tile):
     gl = _every_placement_circuit(n, seed=n)
     c = build_circuit(gl, n)
