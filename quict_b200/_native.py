@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libqsim.so")
+# QSIM_LIB overrides the library path (e.g. an instrumented build)
+LIB_PATH = os.environ.get("QSIM_LIB") or os.path.join(_HERE, "libqsim.so")
 
 # ---- constants mirrored from include/qsim.h --------------------------------
 QS_OK, QS_EINVAL, QS_ECUDA, QS_EWORKSPACE, QS_ENOTSUP, QS_ETIMEOUT = 0, -1, -2, -3, -4, -5

@@ -542,6 +542,12 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     V* msm = bufs[1] + (size_t(1) << K);
     uint64_t* hoff = reinterpret_cast<uint64_t*>(msm + p.nmats);
     uint64_t* gslot_store = hoff + (size_t(1) << H);  // E entries: global offset of each slot
+    // op and stage descriptors live in shared memory: the per-op loop reads
+    // them with a data-dependent index, which the constant cache serves poorly
+    KOp* sops = reinterpret_cast<KOp*>(gslot_store + E);
+    KStage* sst = reinterpret_cast<KStage*>(sops + p.nops);
+    for (int o = threadIdx.x; o < p.nops; o += blockDim.x) sops[o] = p.ops[o];
+    for (int o = threadIdx.x; o < p.nstages; o += blockDim.x) sst[o] = p.st[o];
     // stage the pass's matrices in slot order; tile high-bit offsets
     for (int o = 0; o < p.nops; ++o) {
         const KCopy& c = p.cp[o];
@@ -591,18 +597,18 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
         if (tile + gridDim.x < ntiles) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + gridDim.x), K, L, hoff);
         V x[E];
         // shared memory -> registers in the first stage's (plain) layout
-        Addr<R> ad = stage_addr<V, R>(p.st[0], nT, false);
+        Addr<R> ad = stage_addr<V, R>(sst[0], nT, false);
         sfor<E>([&](auto sc) __attribute__((always_inline)) {
             constexpr int s = decltype(sc)::value;
             x[s] = cur[ad.template at<s>()];
         });
         for (int si = 0; si < p.nstages; ++si) {
-            const KStage& S = p.st[si];
-            if (si > 0) ad = r_relayout<V, R>(x, cur, p.st[si - 1], S, nT);
+            const KStage& S = sst[si];
+            if (si > 0) ad = r_relayout<V, R>(x, cur, sst[si - 1], S, nT);
             const uint32_t thr = thread_bits<R>(S, nT);
             const int oe = S.op_begin + S.op_count;
             for (int o = S.op_begin; o < oe; ++o) {
-                const KOp& op = p.ops[o];
+                const KOp& op = sops[o];
                 if ((base & op.gctrl) != op.gctrl) continue;
                 if ((thr & op.tctrl) != op.tctrl) continue;
                 r_apply<V, R>(x, op, msm, thr, base, cur, ad);
@@ -847,7 +853,8 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
             set_error("qs_apply_fused: op %d does not fit a register tile", ps.op_begin + first);
             return QS_EINVAL;
         }
-        size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R));
+        size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
+                      sizeof(KOp) * args.nops + sizeof(KStage) * args.nstages;
         uint64_t ntiles = uint64_t(1) << (n - ps.k);
         uint64_t cap = uint64_t(sm_count());
         k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), 1 << (ps.k - R), smem, st>>>(vec, args, mats);
@@ -864,7 +871,8 @@ template <typename V>
 int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
     constexpr int R = reg_bits<V>();
     const int nT = ps.k - R;
-    const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R));
+    const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
+                        sizeof(KOp) * QS_MAX_PASS_OPS + sizeof(KStage) * kMaxStages;
     if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
     return launch_smem<V>(vec, n, ps, ops, mats, st);
 }

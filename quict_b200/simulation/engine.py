@@ -53,8 +53,9 @@ class Workspace:
 
 class Engine:
     def __init__(self, device: torch.device, fusion: bool = True, tile_bits: Optional[int] = None,
-                 low_bits: Optional[int] = None, max_pass_cost: float = float("inf")):
+                 low_bits: Optional[int] = None, max_pass_cost: float = float("inf"), merge_bits: int = 2):
         self.device = device
+        self.merge_bits = merge_bits
         self.fusion = fusion
         self.tile_bits = tile_bits
         self.low_bits = low_bits
@@ -101,7 +102,7 @@ class Engine:
 
     def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
         k, nlow = self.tile_shape(vec)
-        return plan(ops, n, k, nlow, max_cost=self.max_pass_cost)
+        return plan(ops, n, k, nlow, max_cost=self.max_pass_cost, merge_bits=self.merge_bits)
 
     def run_passes(self, vec: torch.Tensor, n: int, passes: List[Pass]):
         if not passes:

@@ -58,11 +58,13 @@ def default_tile(dtype_bytes: int) -> Tuple[int, int]:
 
 
 def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_PASS_OPS,
-         max_cost: float = float("inf")) -> List[Step]:
+         max_cost: float = float("inf"), merge_bits: int = 0) -> List[Step]:
     """Greedy in-order planner with commutation-aware hoisting.
 
     ``max_cost`` bounds the per-pass arithmetic, measured in dense-1q-gate
     equivalents (see ``op_cost``), so that a pass stays bandwidth-bound.
+    ``merge_bits`` > 0 multiplies runs of ops on at most that many tile bits
+    into single ops (``merge_ops``).
     """
     k = min(k, n)
     nlow = min(nlow, k)
@@ -117,9 +119,102 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
             if b not in hi:
                 hi.add(b)
             b += 1
+        if merge_bits > 0:
+            chosen = merge_ops(chosen, frozenset(range(nlow)) | frozenset(hi), merge_bits)
         steps.append(Pass(k, nlow, tuple(sorted(hi)), chosen))
         pending = deferred
     return steps
+
+
+def _embed(u: np.ndarray, bits: Tuple[int, ...], into: Tuple[int, ...]) -> np.ndarray:
+    """Matrix `u` acting big-endian on `bits`, expressed on `into` (a superset)."""
+    k, m = len(into), len(bits)
+    if tuple(bits) == tuple(into):
+        return u
+    full = np.kron(u, np.eye(1 << (k - m), dtype=np.complex128))  # order: bits, then the rest
+    order = list(bits) + [b for b in into if b not in bits]
+    # permute tensor axes from `order` to `into`
+    perm = [order.index(b) for b in into]
+    t = full.reshape([2] * (2 * k))
+    t = np.transpose(t, perm + [k + p for p in perm])
+    return t.reshape(1 << k, 1 << k)
+
+
+def _full_matrix(op: Op) -> Tuple[Tuple[int, ...], np.ndarray]:
+    """(bits, matrix) of an op with its controls folded in (controls first)."""
+    u = op.dense()
+    bits = tuple(op.cbits) + tuple(op.tbits)
+    if op.cbits:
+        d = u.shape[0] << len(op.cbits)
+        full = np.eye(d, dtype=np.complex128)
+        full[d - u.shape[0]:, d - u.shape[0]:] = u
+        u = full
+    return bits, u
+
+
+def _to_op(bits: Tuple[int, ...], u: np.ndarray) -> Op:
+    from .lowering import classify
+    kind = classify(u)
+    if kind == "diag":
+        return Op("diag", tuple(bits), (), np.diag(u).copy())
+    return Op(kind, tuple(bits), (), u)
+
+
+def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2) -> List[Op]:
+    """Multiply runs of ops that act on at most `max_bits` tile-resident bits
+    into single ops (gate fusion at the matrix level).
+
+    Open blocks hold disjoint bit sets, so they commute with each other; an op
+    that touches several blocks closes them (emits them) first, and an op that
+    cannot be merged (bits outside the tile, too many bits, tagged for
+    gradients) closes the blocks it touches and is emitted as is.  Order is
+    therefore preserved between every pair of ops that share a bit."""
+    out: List[Op] = []
+    blocks: List[list] = []  # [bits tuple, matrix, [source ops]]
+
+    def close(b):
+        blocks.remove(b)
+        if len(b[2]) == 1:
+            out.append(b[2][0])
+        else:
+            out.append(_to_op(b[0], b[1]))
+
+    for op in ops:
+        S = set(op.tbits) | set(op.cbits)
+        hit = [b for b in blocks if S & set(b[0])]
+        mergeable = op.tag is None and S <= tile and len(S) <= max_bits
+        union = set(S)
+        for b in hit:
+            union |= set(b[0])
+        if not mergeable or len(union) > max_bits:
+            for b in hit:
+                close(b)
+            if mergeable:
+                bits, u = _full_matrix(op)
+                blocks.append([bits, u, [op]])
+            else:
+                out.append(op)
+            continue
+        # merge the hit blocks (disjoint, commuting) and the op into one block
+        if hit:
+            bits: Tuple[int, ...] = ()
+            u = np.eye(1, dtype=np.complex128)
+            srcs: List[Op] = []
+            for b in hit:
+                nb = bits + tuple(x for x in b[0] if x not in bits)
+                u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
+                bits = nb
+                srcs += b[2]
+                blocks.remove(b)
+        else:
+            bits, u, srcs = (), np.eye(1, dtype=np.complex128), []
+        ob, ou = _full_matrix(op)
+        nb = bits + tuple(x for x in ob if x not in bits)
+        u = _embed(ou, ob, nb) @ _embed(u, bits, nb)
+        blocks.append([nb, u, srcs + [op]])
+    for b in list(blocks):
+        close(b)
+    return out
 
 
 def op_entries(op: Op) -> int:

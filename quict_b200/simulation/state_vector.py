@@ -69,7 +69,7 @@ class StateVectorSimulator:
     def __init__(self, device: str = "GPU", precision: str = "double", gpu_device_id: int = 0,
                  matrix_aggregation: bool = True, sync: bool = True, *, fusion: bool = True,
                  tile_bits: Optional[int] = None, low_bits: Optional[int] = None,
-                 max_pass_cost: float = float("inf"), legacy_2q_order: bool = False,
+                 max_pass_cost: float = float("inf"), merge_bits: int = 2, legacy_2q_order: bool = False,
                  seed: Optional[int] = None):
         if device not in self.__DEVICE:
             raise ValueError(f"StateVectorSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
@@ -84,7 +84,7 @@ class StateVectorSimulator:
         self._legacy = legacy_2q_order
         self._tdev = require_cuda(gpu_device_id)
         self._engine = Engine(self._tdev, fusion=fusion, tile_bits=tile_bits, low_bits=low_bits,
-                              max_pass_cost=max_pass_cost)
+                              max_pass_cost=max_pass_cost, merge_bits=merge_bits)
         # measurement uniforms: a seed, or any object with a .random() method
         self._rng = seed if hasattr(seed, "random") else np.random.default_rng(seed)
         self._circuit = None

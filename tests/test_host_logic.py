@@ -80,11 +80,12 @@ def test_legacy_order_reverses_only_uncontrolled_dense():
 
 @pytest.mark.parametrize("seed", range(6))
 @pytest.mark.parametrize("k,nlow", [(3, 1), (4, 2), (5, 5), (4, 0)])
-def test_fusion_plan_preserves_semantics(seed, k, nlow):
+@pytest.mark.parametrize("merge", [0, 2, 3])
+def test_fusion_plan_preserves_semantics(seed, k, nlow, merge):
     """Executing the planner's passes in order equals the original order."""
     from quict_b200.simulation.fusion import Pass, Single, plan
     c, ops = _all_ops(6, seed)
-    steps = plan(ops, 6, k, nlow, max_ops=7)
+    steps = plan(ops, 6, k, nlow, max_ops=7, merge_bits=merge)
     flat = []
     for s in steps:
         if isinstance(s, Pass):
@@ -95,7 +96,8 @@ def test_fusion_plan_preserves_semantics(seed, k, nlow):
             flat.extend(s.ops)
         else:
             flat.append(s.op)
-    assert sorted(map(id, flat)) == sorted(map(id, ops))
+    if not merge:
+        assert sorted(map(id, flat)) == sorted(map(id, ops))
     ref = _apply_ops_oracle(osv.zero_state(6), 6, ops)
     got = _apply_ops_oracle(osv.zero_state(6), 6, flat)
     np.testing.assert_allclose(got, ref, atol=1e-12)
@@ -183,3 +185,20 @@ def test_abi_validation_without_gpu():
     ops[0].gbit[0], ops[0].tgt[0] = 5, 2
     ops[0].mat = 1  # 4 entries needed from offset 1 in a 4-entry table
     assert lib.qs_apply_fused(fake, 8, N.QS_C128, ps, 1, ops, 1, fake, 4, None) == N.QS_EINVAL
+
+
+def test_merge_ops_reduces_op_count_and_keeps_kinds():
+    from quict_b200.core import Circuit, H, Rz, CX, X
+    from quict_b200.simulation.fusion import merge_ops
+    from quict_b200.simulation.lowering import lower_circuit
+    n = 6
+    c = Circuit(n)
+    H | c(0); Rz(0.3) | c(0); H | c(0); CX | c([0, 1]); Rz(0.2) | c(1)
+    X | c(4)                     # alone: keeps its anti-diagonal kind
+    ops = lower_circuit(c.gates, n)
+    merged = merge_ops(ops, frozenset(range(n)), 2)
+    assert len(merged) == 2
+    assert any(o.kind == "antidiag" and o.tbits == (1,) for o in merged)
+    ref = _apply_ops_oracle(osv.zero_state(n), n, ops)
+    got = _apply_ops_oracle(osv.zero_state(n), n, merged)
+    np.testing.assert_allclose(got, ref, atol=1e-13)
