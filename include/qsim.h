@@ -60,8 +60,12 @@ extern "C" {
 #define QS_OP_DIAG  2     /* diagonal on m bits anywhere in the vector         */
 #define QS_OP_ANTI  3     /* m = 1: anti-diagonal 2x2 (entries m01, m10 used)   */
 #define QS_OP_SWAP  4     /* m = 2: swap-like 4x4 (m00, m12, m21, m33 used)     */
+#define QS_OP_EXPECT 5    /* qs_adjoint_fused only: partial <lam| G |psi> over the
+                             tile for a generator G (m <= 2, dense, or diagonal
+                             with QS_OPF_DIAG), summed into partials[slot]     */
 #define QS_MAX_PASS_MATS 2048  /* matrix entries one pass may reference        */
 #define QS_OPF_UNIT 1     /* ANTI: m01 = m10 = 1; SWAP: m00 = m12 = m21 = m33 = 1 */
+#define QS_OPF_DIAG 2     /* EXPECT: the generator is diagonal (2^m entries)   */
 
 /* ---- probability sources and sampling modes ------------------------------ */
 #define QS_SRC_SV  0      /* p_i = |vec[i]|^2                                  */
@@ -73,7 +77,7 @@ extern "C" {
 #define QS_MAX_TILE_BITS 14
 #define QS_MAX_PASS_OPS  160
 
-/* One op of a fused pass.  64 bytes, plain old data (mirrored by ctypes). */
+/* One op of a fused pass.  80 bytes, plain old data (mirrored by ctypes). */
 typedef struct qs_op {
     int32_t  kind;       /* QS_OP_MAT, QS_OP_DIAG, QS_OP_ANTI or QS_OP_SWAP     */
     int32_t  m;          /* number of target bits, 1..4                         */
@@ -85,16 +89,24 @@ typedef struct qs_op {
     uint64_t gctrl;      /* control mask on vector bits outside the tile        */
     int64_t  mat;        /* element offset of the op's matrix in the table
                             (QS_OP_DIAG: 2^m entries, the other kinds: 4^m)    */
+    int64_t  mat_stride; /* batched passes: instance i uses mat + i*mat_stride  */
+    int32_t  slot;       /* QS_OP_EXPECT: output slot                          */
+    int32_t  pad1;
 } qs_op;
 
 /* One fused pass: a tile of 2^k amplitudes made of vector bits 0..nlow-1 and
- * hi[0..k-nlow-1] (ascending), and ops [op_begin, op_begin+op_count). */
+ * hi[0..k-nlow-1] (ascending), and ops [op_begin, op_begin+op_count).
+ * Batched state (inst_shift > 0): the vector holds instances of 2^inst_shift
+ * amplitudes; instance = index >> inst_shift.  All tile bits must be below
+ * inst_shift, so a tile belongs to one instance. */
 typedef struct qs_pass {
     int32_t k;
     int32_t nlow;
     int32_t hi[QS_MAX_TILE_BITS];
     int32_t op_begin;
     int32_t op_count;
+    int32_t inst_shift;
+    int32_t pad;
 } qs_pass;
 
 /* ---- library ------------------------------------------------------------ */
@@ -147,6 +159,32 @@ int qs_apply_kq(void* vec, int n, int dtype, int k, const int32_t* bits,
 int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes, int npasses,
                    const qs_op* ops, int64_t nops_total, const void* mats_dev,
                    int64_t mats_count, void* stream);
+
+/* ---- differentiation / observables ---------------------------------------- */
+/* Backward-sweep pass of the adjoint method: every QS_OP_MAT / DIAG / ANTI /
+ * SWAP op is applied to BOTH psi and lam (the caller passes the inverse
+ * gates), and every QS_OP_EXPECT op adds the tile's partial sum of
+ * conj(lam_i) (G psi)_i to partials[2 * (slot * ntiles + tile)] (re, im; FP64),
+ * ntiles = 2^(n - k) of the pass.  partials_count bounds the slots*ntiles.
+ * Replaces per-parameter circuit re-runs (parameter shift); the reference has
+ * no gradient path (its ML package is not part of it). */
+int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs_pass* passes, int npasses,
+                     const qs_op* ops, int64_t nops_total, const void* mats_dev, int64_t mats_count,
+                     double* partials_dev, int64_t partials_count, void* stream);
+
+/* out = sum_t c_t P_t psi for Pauli strings P_t = i^popc(x&z) X^x Z^z (x, z:
+ * HOST arrays of masks over vector bits, coeff: HOST complex128 pairs).  out
+ * and psi must not alias.  Used for lam = H psi. */
+int qs_apply_pauli_sum(const void* psi, void* out, int n, int dtype, const uint64_t* xmask,
+                       const uint64_t* zmask, const double* coeff, int nterms, void* stream);
+
+/* out_dev[2*i] + i*out_dev[2*i+1] = sum over instance i of conj(a_j) b_j
+ * (FP64), instances of 2^inst_bits amplitudes.  ws: qs_reduce_ws_bytes. */
+int qs_inner_batched(const void* a, const void* b, int n, int dtype, int inst_bits, double* out_dev,
+                     void* ws, size_t ws_bytes, void* stream);
+
+/* out[s] = sum_{t < seglen} in[s * seglen + t] for complex FP64 pairs. */
+int qs_segment_sum(const double* in_dev, int64_t nseg, int64_t seglen, double* out_dev, void* stream);
 
 /* ---- measurement, reset, sampling ------------------------------------------ */
 size_t qs_reduce_ws_bytes(int n);

@@ -20,7 +20,8 @@ QS_OK, QS_EINVAL, QS_ECUDA, QS_EWORKSPACE, QS_ENOTSUP, QS_ETIMEOUT = 0, -1, -2, 
 QS_C64, QS_C128 = 0, 1
 QS_K_DENSE, QS_K_DIAG, QS_K_ANTIDIAG, QS_K_SWAP = 0, 1, 2, 3
 QS_OP_MAT, QS_OP_DIAG, QS_OP_ANTI, QS_OP_SWAP = 1, 2, 3, 4
-QS_OPF_UNIT = 1
+QS_OP_EXPECT = 5
+QS_OPF_UNIT, QS_OPF_DIAG = 1, 2
 QS_MAX_PASS_MATS = 2048
 QS_SRC_SV, QS_SRC_DM = 0, 1
 QS_SAMPLE_CDF, QS_SAMPLE_SEQ = 0, 1
@@ -50,6 +51,9 @@ class qs_op(C.Structure):
         ("flags", C.c_uint32),
         ("gctrl", C.c_uint64),
         ("mat", C.c_int64),
+        ("mat_stride", C.c_int64),
+        ("slot", C.c_int32),
+        ("pad1", C.c_int32),
     ]
 
 
@@ -60,11 +64,13 @@ class qs_pass(C.Structure):
         ("hi", C.c_int32 * QS_MAX_TILE_BITS),
         ("op_begin", C.c_int32),
         ("op_count", C.c_int32),
+        ("inst_shift", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
-assert C.sizeof(qs_op) == 64
-assert C.sizeof(qs_pass) == 8 + 4 * QS_MAX_TILE_BITS + 8
+assert C.sizeof(qs_op) == 80
+assert C.sizeof(qs_pass) == 8 + 4 * QS_MAX_TILE_BITS + 16
 
 _vp, _i, _i64, _u64, _d, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
 _dp = C.POINTER(C.c_double)
@@ -81,6 +87,11 @@ SIGNATURES = {
     "qs_apply_2q": (_i, [_vp, _i, _i, _i, _i, _u64, _i, _dp, _vp]),
     "qs_apply_kq": (_i, [_vp, _i, _i, _i, _i32p, _u64, _vp, _vp]),
     "qs_apply_fused": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp]),
+    "qs_adjoint_fused": (_i, [_vp, _vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp,
+                              _i64, _vp]),
+    "qs_apply_pauli_sum": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp]),
+    "qs_inner_batched": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp, _sz, _vp]),
+    "qs_segment_sum": (_i, [_vp, _i64, _i64, _vp, _vp]),
     "qs_reduce_ws_bytes": (_sz, [_i]),
     "qs_prob0": (_i, [_vp, _i, _i, _i, _i, _vp, _sz, _vp, _vp]),
     "qs_norm2": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp, _vp]),

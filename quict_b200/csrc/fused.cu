@@ -72,7 +72,7 @@ __device__ __forceinline__ uint32_t ins0(uint32_t x, int b) {
 
 // =============================================================== shared-memory kernel
 struct PassArgs {
-    int n, k, nlow, nops;
+    int n, k, nlow, nops, inst_shift;
     int hi[QS_MAX_TILE_BITS];
     qs_op ops[QS_MAX_PASS_OPS];
 };
@@ -150,14 +150,90 @@ __device__ __forceinline__ void tile_diag(V* __restrict__ tile, int K, uint64_t 
     }
 }
 
+// <lam| G |psi> over the tile for a generator on m <= 2 tile bits (dense) or
+// a diagonal on bits anywhere (QS_OPF_DIAG); thread-partial sum returned.
+template <typename V, int M>
+__device__ __forceinline__ double2 tile_expect_dense(const V* __restrict__ psi, const V* __restrict__ lam, int K,
+                                                     const qs_op& op, const V* __restrict__ g) {
+    constexpr int D = 1 << M;
+    int t[M], s[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) t[j] = op.tgt[j];
+    sort_bits<M>(t, s);
+    uint32_t spread[D];
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+        uint32_t o = 0;
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+            if ((r >> (M - 1 - j)) & 1) o |= 1u << t[j];
+        spread[r] = o;
+    }
+    double re = 0.0, im = 0.0;
+    const uint32_t groups = 1u << (K - M);
+    for (uint32_t gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+        uint32_t i0 = gi;
+#pragma unroll
+        for (int j = 0; j < M; ++j) i0 = ins0(i0, s[j]);
+        if ((i0 & op.lctrl) != op.lctrl) continue;
+        V x[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r) x[r] = psi[i0 | spread[r]];
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            V acc = cmul(g[r * D], x[0]);
+#pragma unroll
+            for (int c = 1; c < D; ++c) acc = cfma(g[r * D + c], x[c], acc);
+            const V l = lam[i0 | spread[r]];
+            re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
+            im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+        }
+    }
+    return make_double2(re, im);
+}
+
 template <typename V>
-__global__ void __launch_bounds__(kFT) k_fused_smem(V* __restrict__ vec, const __grid_constant__ PassArgs p,
-                                                     const V* __restrict__ mats) {
+__device__ __forceinline__ double2 tile_expect_diag(const V* __restrict__ psi, const V* __restrict__ lam, int K,
+                                                    uint64_t base, const qs_op& op, const V* __restrict__ d) {
+    const int m = op.m;
+    uint32_t ext = 0;
+    int lpos[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        lpos[j] = -1;
+        if (j < m) {
+            if (op.tgt[j] < 0) ext |= uint32_t((base >> op.gbit[j]) & 1) << (m - 1 - j);
+            else lpos[j] = op.tgt[j];
+        }
+    }
+    double re = 0.0, im = 0.0;
+    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
+        if ((e & op.lctrl) != op.lctrl) continue;
+        uint32_t sidx = ext;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < m && lpos[j] >= 0) sidx |= ((e >> lpos[j]) & 1u) << (m - 1 - j);
+        const V acc = cmul(d[sidx], psi[e]);
+        const V l = lam[e];
+        re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
+        im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+    }
+    return make_double2(re, im);
+}
+
+// Shared-memory tile kernel.  ADJ: two vectors (psi, lam) move through the
+// same tiles; apply-ops act on both and EXPECT ops write per-tile partials.
+template <typename V, bool ADJ>
+__global__ void __launch_bounds__(kFT) k_fused_smem(V* __restrict__ vec, V* __restrict__ vec2,
+                                                     const __grid_constant__ PassArgs p, const V* __restrict__ mats,
+                                                     double* __restrict__ partials) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double2 red[kFT / 32];
     const int K = p.k, L = p.nlow, H = K - L;
     const uint32_t T = 1u << K;
     V* tile = reinterpret_cast<V*>(smem_raw);
-    uint64_t* hoff = reinterpret_cast<uint64_t*>(smem_raw + sizeof(V) * T);
+    V* tile2 = tile + (ADJ ? T : 0);
+    uint64_t* hoff = reinterpret_cast<uint64_t*>(smem_raw + sizeof(V) * T * (ADJ ? 2 : 1));
     for (uint32_t j = threadIdx.x; j < (1u << H); j += kFT) {
         uint64_t o = 0;
         for (int t = 0; t < H; ++t)
@@ -170,25 +246,61 @@ __global__ void __launch_bounds__(kFT) k_fused_smem(V* __restrict__ vec, const _
     for (uint64_t tid = blockIdx.x; tid < ntiles; tid += gridDim.x) {
         uint64_t base = tid << L;
         for (int t = 0; t < H; ++t) base = insert0(base, p.hi[t]);
-        for (uint32_t e = threadIdx.x; e < T; e += kFT) tile[e] = vec[base | hoff[e >> L] | (e & lmask)];
+        const uint64_t inst = p.inst_shift > 0 ? (base >> p.inst_shift) : 0;
+        for (uint32_t e = threadIdx.x; e < T; e += kFT) {
+            const uint64_t gi = base | hoff[e >> L] | (e & lmask);
+            tile[e] = vec[gi];
+            if (ADJ) tile2[e] = vec2[gi];
+        }
         __syncthreads();
         for (int o = 0; o < p.nops; ++o) {
             const qs_op& op = p.ops[o];
-            if ((base & op.gctrl) != op.gctrl) continue;  // CTA-uniform
-            const V* mat = mats + op.mat;
+            const bool on = (base & op.gctrl) == op.gctrl;  // CTA-uniform
+            const V* mat = mats + op.mat + int64_t(inst) * op.mat_stride;
+            if (ADJ && op.kind == QS_OP_EXPECT) {
+                double2 v = make_double2(0.0, 0.0);
+                if (on) {
+                    if (op.flags & QS_OPF_DIAG) v = tile_expect_diag<V>(tile, tile2, K, base, op, mat);
+                    else if (op.m == 1) v = tile_expect_dense<V, 1>(tile, tile2, K, op, mat);
+                    else v = tile_expect_dense<V, 2>(tile, tile2, K, op, mat);
+                }
+                // block reduction in a fixed order (deterministic)
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+                    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+                }
+                if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    double2 s2 = make_double2(0.0, 0.0);
+                    for (int w = 0; w < kFT / 32; ++w) { s2.x += red[w].x; s2.y += red[w].y; }
+                    const uint64_t at = 2 * (uint64_t(op.slot) * ntiles + tid);
+                    partials[at] = s2.x;
+                    partials[at + 1] = s2.y;
+                }
+                __syncthreads();
+                continue;
+            }
+            if (!on) continue;
             if (op.kind == QS_OP_DIAG) {
                 tile_diag<V>(tile, K, base, op, mat);
+                if (ADJ) tile_diag<V>(tile2, K, base, op, mat);
             } else {
                 switch (op.m) {
-                    case 1: tile_mat<V, 1>(tile, K, op, mat); break;
-                    case 2: tile_mat<V, 2>(tile, K, op, mat); break;
-                    case 3: tile_mat<V, 3>(tile, K, op, mat); break;
-                    default: tile_mat<V, 4>(tile, K, op, mat); break;
+                    case 1: tile_mat<V, 1>(tile, K, op, mat); if (ADJ) tile_mat<V, 1>(tile2, K, op, mat); break;
+                    case 2: tile_mat<V, 2>(tile, K, op, mat); if (ADJ) tile_mat<V, 2>(tile2, K, op, mat); break;
+                    case 3: tile_mat<V, 3>(tile, K, op, mat); if (ADJ) tile_mat<V, 3>(tile2, K, op, mat); break;
+                    default: tile_mat<V, 4>(tile, K, op, mat); if (ADJ) tile_mat<V, 4>(tile2, K, op, mat); break;
                 }
             }
             __syncthreads();
         }
-        for (uint32_t e = threadIdx.x; e < T; e += kFT) vec[base | hoff[e >> L] | (e & lmask)] = tile[e];
+        for (uint32_t e = threadIdx.x; e < T; e += kFT) {
+            const uint64_t gi = base | hoff[e >> L] | (e & lmask);
+            vec[gi] = tile[e];
+            if (ADJ) vec2[gi] = tile2[e];
+        }
         __syncthreads();
     }
 }
@@ -210,6 +322,7 @@ struct KOp {
 };
 struct KCopy {
     int64_t goff;     // table offset of the stored matrix
+    int64_t stride;   // per-instance stride (batched passes)
     uint16_t soff;    // shared-memory offset
     uint8_t m;
     uint8_t diag;
@@ -221,7 +334,7 @@ struct KStage {
     uint16_t op_begin, op_count;
 };
 struct RegArgs {
-    int n, K, L, H, nT, nstages, nops, nmats;
+    int n, K, L, H, nT, nstages, nops, nmats, inst_shift, batched;
     int hi[QS_MAX_TILE_BITS];
     KStage st[kMaxStages];
     KOp ops[QS_MAX_PASS_OPS];
@@ -548,21 +661,26 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     KStage* sst = reinterpret_cast<KStage*>(sops + p.nops);
     for (int o = threadIdx.x; o < p.nops; o += blockDim.x) sops[o] = p.ops[o];
     for (int o = threadIdx.x; o < p.nstages; o += blockDim.x) sst[o] = p.st[o];
-    // stage the pass's matrices in slot order; tile high-bit offsets
-    for (int o = 0; o < p.nops; ++o) {
-        const KCopy& c = p.cp[o];
-        const int D = 1 << c.m;
-        const int cnt = c.diag ? D : D * D;
-        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-            const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
-            int sr = 0, sc = 0;
-            for (int i = 0; i < c.m; ++i) {
-                sr |= ((kr >> i) & 1) << c.perm[i];
-                sc |= ((kc >> i) & 1) << c.perm[i];
+    // stage the pass's matrices in slot order (per instance when batched)
+    auto stage_mats = [&](uint64_t inst) {
+        for (int o = 0; o < p.nops; ++o) {
+            const KCopy& c = p.cp[o];
+            const int D = 1 << c.m;
+            const int cnt = c.diag ? D : D * D;
+            const V* src = mats + c.goff + int64_t(inst) * c.stride;
+            for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+                const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
+                int sr = 0, sc = 0;
+                for (int i = 0; i < c.m; ++i) {
+                    sr |= ((kr >> i) & 1) << c.perm[i];
+                    sc |= ((kc >> i) & 1) << c.perm[i];
+                }
+                msm[c.soff + e] = src[c.diag ? sr : sr * D + sc];
             }
-            msm[c.soff + e] = mats[c.goff + (c.diag ? sr : sr * D + sc)];
         }
-    }
+    };
+    uint64_t staged = 0;
+    stage_mats(0);
     for (uint32_t j = threadIdx.x; j < (1u << H); j += blockDim.x) {
         uint64_t o = 0;
         for (int t = 0; t < H; ++t)
@@ -593,8 +711,16 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
         V* cur = bufs[it & 1];
         const uint64_t base = tile_base(tile);
         cp_async_wait_all();
-        __syncthreads();  // tile landed; the other buffer is free
+        __syncthreads();  // tile landed; the other buffer is free; previous tile's ops are done
         if (tile + gridDim.x < ntiles) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + gridDim.x), K, L, hoff);
+        if (p.batched) {
+            const uint64_t inst = base >> p.inst_shift;
+            if (inst != staged) {
+                stage_mats(inst);
+                staged = inst;
+                __syncthreads();
+            }
+        }
         V x[E];
         // shared memory -> registers in the first stage's (plain) layout
         Addr<R> ad = stage_addr<V, R>(sst[0], nT, false);
@@ -625,7 +751,8 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
 }
 
 // ------------------------------------------------------------------ host side
-int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total, int64_t mats_count) {
+int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total, int64_t mats_count,
+                  bool adjoint = false, int64_t partials_count = 0) {
     QS_REQUIRE(ps.k >= 1 && ps.k <= QS_MAX_TILE_BITS && ps.k <= n, "tile bits %d outside [1, min(%d, n)]", ps.k,
                QS_MAX_TILE_BITS);
     QS_REQUIRE(ps.nlow >= 0 && ps.nlow <= ps.k, "nlow %d outside [0, k]", ps.nlow);
@@ -639,13 +766,26 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
         prev = ps.hi[t];
         tilemask |= uint64_t(1) << ps.hi[t];
     }
+    QS_REQUIRE(ps.inst_shift >= 0 && ps.inst_shift <= n, "inst_shift %d outside [0, n]", ps.inst_shift);
+    if (ps.inst_shift > 0)
+        QS_REQUIRE((tilemask >> ps.inst_shift) == 0, "tile bits must lie below inst_shift (one instance per tile)");
+    const int64_t ninst = ps.inst_shift > 0 ? (int64_t(1) << (n - ps.inst_shift)) : 1;
+    const int64_t ntiles = int64_t(1) << (n - ps.k);
     int local[64];
     for (int b = 0; b < 64; ++b) local[b] = -1;
     for (int b = 0; b < ps.nlow; ++b) local[b] = b;
     for (int t = 0; t < ps.k - ps.nlow; ++t) local[ps.hi[t]] = ps.nlow + t;
     for (int i = 0; i < ps.op_count; ++i) {
         const qs_op& op = ops[ps.op_begin + i];
-        QS_REQUIRE(op.kind >= QS_OP_MAT && op.kind <= QS_OP_SWAP, "op %d: bad kind %d", i, op.kind);
+        QS_REQUIRE((op.kind >= QS_OP_MAT && op.kind <= QS_OP_SWAP) || (adjoint && op.kind == QS_OP_EXPECT),
+                   "op %d: bad kind %d", i, op.kind);
+        QS_REQUIRE(op.mat_stride >= 0 && (ps.inst_shift > 0 || op.mat_stride == 0),
+                   "op %d: a per-instance matrix stride needs inst_shift > 0", i);
+        if (op.kind == QS_OP_EXPECT) {
+            QS_REQUIRE(op.m <= 2 || (op.flags & QS_OPF_DIAG), "op %d: dense EXPECT generators act on <= 2 bits", i);
+            QS_REQUIRE(op.slot >= 0 && (int64_t(op.slot) + 1) * ntiles * 2 <= partials_count,
+                       "op %d: EXPECT slot %d outside the partials buffer", i, op.slot);
+        }
         QS_REQUIRE(op.m >= 1 && op.m <= 4, "op %d: m=%d outside [1, 4]", i, op.m);
         QS_REQUIRE(op.kind != QS_OP_ANTI || op.m == 1, "op %d: ANTI needs m = 1", i);
         QS_REQUIRE(op.kind != QS_OP_SWAP || op.m == 2, "op %d: SWAP needs m = 2", i);
@@ -655,45 +795,49 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
         for (int j = 0; j < op.m; ++j) {
             QS_REQUIRE(op.gbit[j] >= 0 && op.gbit[j] < n, "op %d: target bit outside [0, n)", i);
             QS_REQUIRE(op.tgt[j] == local[op.gbit[j]], "op %d: tile position of target %d inconsistent", i, j);
-            if (op.kind != QS_OP_DIAG) QS_REQUIRE(op.tgt[j] >= 0, "op %d: dense target outside the tile", i);
+            const bool diag = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+            if (!diag) QS_REQUIRE(op.tgt[j] >= 0, "op %d: dense target outside the tile", i);
             if (op.tgt[j] >= 0) {
                 QS_REQUIRE(!((tl >> op.tgt[j]) & 1), "op %d: duplicate target", i);
                 tl |= 1u << op.tgt[j];
             }
         }
         QS_REQUIRE((tl & op.lctrl) == 0, "op %d: control overlaps a target", i);
-        int64_t len = op.kind == QS_OP_DIAG ? (int64_t(1) << op.m) : (int64_t(1) << (2 * op.m));
-        QS_REQUIRE(op.mat >= 0 && op.mat + len <= mats_count, "op %d: matrix outside the table", i);
+        const bool dg = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+        int64_t len = dg ? (int64_t(1) << op.m) : (int64_t(1) << (2 * op.m));
+        QS_REQUIRE(op.mat >= 0 && op.mat + (ninst - 1) * op.mat_stride + len <= mats_count,
+                   "op %d: matrix outside the table", i);
     }
     return QS_OK;
 }
 
-template <typename V>
+// Opt a kernel into large dynamic shared memory once per (kernel, device).
 void config_smem(const void* fn) {
-    static int done[64] = {0};
+    static thread_local std::vector<std::pair<const void*, int>> done;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        done[dev] = 1;
-    }
+    for (const auto& d : done)
+        if (d.first == fn && d.second == dev) return;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    done.emplace_back(fn, dev);
 }
 
-template <typename V>
-int launch_smem(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+template <typename V, bool ADJ>
+int launch_smem(V* vec, V* vec2, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials,
+                cudaStream_t st) {
     static thread_local PassArgs args;
-    args.n = n; args.k = ps.k; args.nlow = ps.nlow; args.nops = ps.op_count;
+    args.n = n; args.k = ps.k; args.nlow = ps.nlow; args.nops = ps.op_count; args.inst_shift = ps.inst_shift;
     for (int t = 0; t < QS_MAX_TILE_BITS; ++t) args.hi[t] = t < ps.k - ps.nlow ? ps.hi[t] : 0;
     for (int i = 0; i < ps.op_count; ++i) args.ops[i] = ops[ps.op_begin + i];
-    size_t smem = sizeof(V) * (size_t(1) << ps.k) + sizeof(uint64_t) * (size_t(1) << (ps.k - ps.nlow));
-    config_smem<V>((const void*)k_fused_smem<V>);
+    size_t smem = sizeof(V) * (size_t(1) << ps.k) * (ADJ ? 2 : 1) + sizeof(uint64_t) * (size_t(1) << (ps.k - ps.nlow));
+    config_smem((const void*)k_fused_smem<V, ADJ>);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_smem<V>, kFT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_smem<V, ADJ>, kFT, smem);
     if (occ < 1) occ = 1;
     uint64_t ntiles = uint64_t(1) << (n - ps.k);
     uint64_t cap = uint64_t(sm_count()) * occ;
-    k_fused_smem<V><<<unsigned(ntiles < cap ? ntiles : cap), kFT, smem, st>>>(vec, args, mats);
-    QS_CHECK_LAUNCH("qs_apply_fused(smem)");
+    k_fused_smem<V, ADJ><<<unsigned(ntiles < cap ? ntiles : cap), kFT, smem, st>>>(vec, vec2, args, mats, partials);
+    QS_CHECK_LAUNCH(ADJ ? "qs_adjoint_fused" : "qs_apply_fused(smem)");
     return QS_OK;
 }
 
@@ -703,6 +847,8 @@ int launch_smem(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
 int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegArgs& a) {
     const int K = ps.k, L = ps.nlow, nT = K - R;
     a.n = n; a.K = K; a.L = L; a.H = K - L; a.nT = nT;
+    a.inst_shift = ps.inst_shift;
+    a.batched = 0;
     for (int t = 0; t < QS_MAX_TILE_BITS; ++t) a.hi[t] = t < K - L ? ps.hi[t] : 0;
     const int lowlanes = 5;  // tile bits 0..4 are the lanes of the load/store layout
     auto xbits = [&](const qs_op& op) {
@@ -787,6 +933,8 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegA
         k.scm = uint8_t(scm);
         k.tctrl = uint16_t(tct);
         c.goff = op.mat;
+        c.stride = op.mat_stride;
+        if (op.mat_stride != 0) a.batched = 1;
         c.soff = uint16_t(moff);
         c.m = uint8_t(op.m);
         c.diag = op.kind == QS_OP_DIAG;
@@ -845,7 +993,7 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegA
 template <typename V, int R>
 int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
     static thread_local RegArgs args;
-    config_smem<V>((const void*)k_fused_reg<V, R>);
+    config_smem((const void*)k_fused_reg<V, R>);
     int first = 0;
     while (first < ps.op_count) {
         int used = build_reg(ps, ops, first, n, R, args);
@@ -874,7 +1022,7 @@ int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
     const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
                         sizeof(KOp) * QS_MAX_PASS_OPS + sizeof(KStage) * kMaxStages;
     if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
-    return launch_smem<V>(vec, n, ps, ops, mats, st);
+    return launch_smem<V, false>(vec, nullptr, n, ps, ops, mats, nullptr, st);
 }
 
 }  // namespace
@@ -902,6 +1050,36 @@ extern "C" int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes
         int rc = dtype == QS_C128
                      ? launch_pass<double2>((double2*)vec, n, passes[i], ops, (const double2*)mats_dev, as_stream(stream))
                      : launch_pass<float2>((float2*)vec, n, passes[i], ops, (const float2*)mats_dev, as_stream(stream));
+        if (rc) return rc;
+    }
+    return QS_OK;
+}
+
+extern "C" int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs_pass* passes, int npasses,
+                                const qs_op* ops, int64_t nops_total, const void* mats_dev, int64_t mats_count,
+                                double* partials_dev, int64_t partials_count, void* stream) {
+    QS_REQUIRE(psi != nullptr && lam != nullptr && psi != lam, "psi and lam must be distinct non-null vectors");
+    QS_REQUIRE(n >= 1 && n <= 40, "qubit count %d outside [1, 40]", n);
+    QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
+    QS_REQUIRE(npasses >= 0 && (npasses == 0 || passes != nullptr), "bad pass array");
+    QS_REQUIRE(nops_total >= 0 && (nops_total == 0 || ops != nullptr), "bad op array");
+    QS_REQUIRE(mats_count >= 0 && (mats_count == 0 || mats_dev != nullptr), "bad matrix table");
+    QS_REQUIRE(partials_count >= 0 && (partials_count == 0 || partials_dev != nullptr), "bad partials buffer");
+    size_t vsize = dtype == QS_C128 ? 16 : 8;
+    for (int i = 0; i < npasses; ++i) {
+        int rc = validate_pass(passes[i], n, ops, nops_total, mats_count, true, partials_count);
+        if (rc) return rc;
+        size_t smem = 2 * vsize * (size_t(1) << passes[i].k) + 8 * (size_t(1) << (passes[i].k - passes[i].nlow));
+        QS_REQUIRE(smem <= 160 * 1024, "pass %d: two tiles of 2^%d need %zu bytes of shared memory", i,
+                   passes[i].k, smem);
+    }
+    for (int i = 0; i < npasses; ++i) {
+        if (passes[i].op_count == 0) continue;
+        int rc = dtype == QS_C128
+                     ? launch_smem<double2, true>((double2*)psi, (double2*)lam, n, passes[i], ops,
+                                                  (const double2*)mats_dev, partials_dev, as_stream(stream))
+                     : launch_smem<float2, true>((float2*)psi, (float2*)lam, n, passes[i], ops,
+                                                 (const float2*)mats_dev, partials_dev, as_stream(stream));
         if (rc) return rc;
     }
     return QS_OK;

@@ -1,0 +1,251 @@
+"""Batched expectation values and adjoint-method gradients on the GPU.
+
+B parameter sets of an n-qubit ``ParamCircuit`` are simulated as ONE vector of
+2^(n + log2 B') amplitudes (B' = B rounded up to a power of two): instance i
+occupies amplitudes [i 2^n, (i+1) 2^n), gates act on the low n bits and each
+parameterised gate reads its instance's matrix through a per-instance stride,
+so a fused pass advances every instance at once.
+
+  forward   psi = U(theta)|0>                       (fused passes, qs_apply_fused)
+            lam = H psi                             (qs_apply_pauli_sum)
+            E   = <psi|lam> per instance            (qs_inner_batched, FP64)
+  backward  for gates k = L..1 (fused into tile passes, qs_adjoint_fused):
+              g_k += scale_k * Im <lam| G_k |psi>   (per-tile FP64 partials)
+              psi <- U_k^dagger psi,  lam <- U_k^dagger lam
+            partials -> per (gate, instance) sums   (qs_segment_sum)
+
+With U(theta) = exp(-i theta G / 2), dE/dtheta_k = 2 Re <lam_k| dU_k |psi_{k-1}>
+= scale_k * Im <lam_k| G_k |psi_k>.  ``parameter_shift`` computes the same
+gradient from 2 * P shifted forward runs (the baseline the adjoint is compared
+against).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from ..simulation.engine import Workspace, qs_dtype, require_cuda
+from ..simulation.fusion import MatrixTable, Pass, Single, default_tile, emit, plan
+from ..simulation.lowering import Op, classify
+from .circuit import GENERATORS, ParamCircuit, PauliSum, rotation
+
+
+def _pow2(b: int) -> int:
+    p = 1
+    while p < b:
+        p <<= 1
+    return p
+
+
+def _batched_rotations(kind: str, thetas: np.ndarray, inverse: bool = False) -> Tuple[str, np.ndarray]:
+    """Per-instance exp(-i t G/2) tables: ("diag", (B, 2^m)) or ("mat", (B, 4^m))."""
+    g = GENERATORS[kind]
+    t = -thetas if inverse else thetas
+    c = np.cos(t / 2)[:, None]
+    s = np.sin(t / 2)[:, None]
+    if classify(g) == "diag":
+        d = np.diag(g)[None, :]
+        return "diag", c - 1j * s * d
+    eye = np.eye(g.shape[0]).ravel()[None, :]
+    return "mat", c * eye - 1j * s * g.ravel()[None, :]
+
+
+class BatchedAdjoint:
+    """Energies and gradients of <psi(theta)|H|psi(theta)> for a batch of theta."""
+
+    def __init__(self, circuit: ParamCircuit, observable: PauliSum, precision: str = "single",
+                 device_id: int = 0, tile_bits: Optional[int] = None):
+        if observable.n != circuit.n:
+            raise ValueError("observable and circuit act on different qubit counts")
+        self.circuit = circuit
+        self.obs = observable
+        self.n = circuit.n
+        self.dev = require_cuda(device_id)
+        self.cdtype = torch.complex64 if precision == "single" else torch.complex128
+        self.np_dtype = np.complex64 if precision == "single" else np.complex128
+        k0, _ = default_tile(8 if precision == "single" else 16)
+        # the adjoint pass keeps two tiles (psi, lam) on chip
+        self.k = min(tile_bits or (k0 - 1), self.n)
+        self.nlow = min(5, self.k)
+        self.ws = Workspace(self.dev)
+        self.launches = 0
+        self.pauli = observable.masks()
+        self._param_entries = [i for i, e in enumerate(circuit.entries) if e.kind != "fixed"]
+
+    # ---- helpers ---------------------------------------------------------------------------
+    @property
+    def stream(self):
+        return N.stream_ptr(torch.cuda.current_stream(self.dev))
+
+    def _vbits(self, qubits: Sequence[int]) -> Tuple[int, ...]:
+        return tuple(self.n - 1 - q for q in qubits)
+
+    def _gate_ops(self, params: np.ndarray, inverse: bool) -> List[Tuple[int, Op]]:
+        """[(entry index, op)] in circuit order; per-instance tables for rotations."""
+        out = []
+        for i, e in enumerate(self.circuit.entries):
+            tb = self._vbits(e.qubits)
+            if e.kind == "fixed":
+                m = np.conj(e.matrix.T) if inverse else e.matrix
+                k = classify(m)
+                out.append((i, Op("diag", tb, (), np.diag(m).copy()) if k == "diag" else Op(k, tb, (), m.copy())))
+            else:
+                kind, tab = _batched_rotations(e.kind, e.scale * params[:, e.index], inverse)
+                m0 = tab[0].copy() if kind == "diag" else tab[0].reshape(1 << len(tb), -1)
+                out.append((i, Op(kind, tb, (), m0, tag=("param", i), batch=tab)))
+        return out
+
+    def _run(self, vec: torch.Tensor, nbits: int, ops: Sequence[Op], lam: Optional[torch.Tensor] = None,
+             partials: Optional[torch.Tensor] = None):
+        steps = plan(ops, nbits, self.k, self.nlow, merge_bits=0 if lam is not None else 2)
+        passes = [s for s in steps if isinstance(s, Pass)]
+        if len(passes) != len(steps):
+            raise RuntimeError("a gradient-circuit op could not be fused")
+        table = MatrixTable()
+        cps, npass, cops, nops = emit(passes, table, inst_shift=self.n)
+        mats = torch.from_numpy(table.array().astype(self.np_dtype)).to(self.dev)
+        if lam is None:
+            N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), nbits, qs_dtype(vec), cps, npass, cops, nops,
+                   C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+        else:
+            N.call("qs_adjoint_fused", C.c_void_p(vec.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
+                   qs_dtype(vec), cps, npass, cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
+                   C.c_void_p(partials.data_ptr()), int(partials.numel()), self.stream)
+        self.launches += npass
+        self._keep = mats
+
+    def _prepare(self, params) -> Tuple[np.ndarray, int, int]:
+        p = params.detach().cpu().numpy() if isinstance(params, torch.Tensor) else np.asarray(params)
+        p = np.atleast_2d(np.asarray(p, dtype=np.float64))
+        if p.shape[1] < self.circuit.num_params:
+            raise ValueError(f"expected {self.circuit.num_params} parameters per instance, got {p.shape[1]}")
+        b = p.shape[0]
+        bp = _pow2(b)
+        if bp != b:
+            p = np.concatenate([p, np.zeros((bp - b, p.shape[1]))], axis=0)
+        return p, b, bp
+
+    def _zero_states(self, bp: int) -> torch.Tensor:
+        vec = torch.zeros(bp << self.n, dtype=self.cdtype, device=self.dev)
+        vec.view(bp, 1 << self.n)[:, 0] = 1
+        return vec
+
+    # ---- public API --------------------------------------------------------------------------
+    def states(self, params) -> torch.Tensor:
+        """Final states, shape (B, 2^n)."""
+        p, b, bp = self._prepare(params)
+        nbits = self.n + (bp.bit_length() - 1)
+        vec = self._zero_states(bp)
+        self._run(vec, nbits, [op for _, op in self._gate_ops(p, False)])
+        return vec.view(bp, 1 << self.n)[:b]
+
+    def _energy(self, psi: torch.Tensor, nbits: int, bp: int) -> Tuple[torch.Tensor, torch.Tensor]:
+        lam = torch.empty_like(psi)
+        x, z, c = self.pauli
+        N.call("qs_apply_pauli_sum", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
+               qs_dtype(psi), x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
+               c.ctypes.data_as(C.c_void_p), len(x), self.stream)
+        e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
+        ws = self.ws.get(16 * bp * 64 + 256)
+        N.call("qs_inner_batched", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits, qs_dtype(psi),
+               self.n, C.c_void_p(e.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(), self.stream)
+        self.launches += 2
+        return lam, e.view(bp, 2)[:, 0]
+
+    def energies(self, params) -> torch.Tensor:
+        p, b, bp = self._prepare(params)
+        nbits = self.n + (bp.bit_length() - 1)
+        psi = self._zero_states(bp)
+        self._run(psi, nbits, [op for _, op in self._gate_ops(p, False)])
+        _, e = self._energy(psi, nbits, bp)
+        return e[:b]
+
+    def gradient(self, params) -> Tuple[torch.Tensor, torch.Tensor]:
+        """(energies (B,), gradients (B, P)) in FP64."""
+        p, b, bp = self._prepare(params)
+        nbits = self.n + (bp.bit_length() - 1)
+        psi = self._zero_states(bp)
+        self._run(psi, nbits, [op for _, op in self._gate_ops(p, False)])
+        lam, e = self._energy(psi, nbits, bp)
+        # backward sweep: EXPECT(G_k) then U_k^dagger, k = L..1
+        inv = self._gate_ops(p, True)
+        slot_of = {entry: s for s, entry in enumerate(self._param_entries)}
+        ops: List[Op] = []
+        for entry, op in reversed(inv):
+            ent = self.circuit.entries[entry]
+            if ent.kind != "fixed":
+                g = GENERATORS[ent.kind]
+                ops.append(Op("expect", op.tbits, (), g, tag=("expect", entry), slot=slot_of[entry]))
+            ops.append(op)
+        nslots = max(1, len(self._param_entries))
+        ntiles = 1 << (nbits - self.k)
+        partials = torch.empty(2 * nslots * ntiles, dtype=torch.float64, device=self.dev)
+        self._run(psi, nbits, ops, lam=lam, partials=partials)
+        per_inst_tiles = 1 << (self.n - self.k)
+        sums = torch.empty(2 * nslots * bp, dtype=torch.float64, device=self.dev)
+        N.call("qs_segment_sum", C.c_void_p(partials.data_ptr()), nslots * bp, per_inst_tiles,
+               C.c_void_p(sums.data_ptr()), self.stream)
+        self.launches += 1
+        im = sums.view(nslots, bp, 2)[:, :, 1]  # Im <lam|G|psi> per (slot, instance)
+        scale = torch.tensor([self.circuit.entries[e].scale for e in self._param_entries], dtype=torch.float64,
+                             device=self.dev)
+        index = torch.tensor([self.circuit.entries[e].index for e in self._param_entries], dtype=torch.long,
+                             device=self.dev)
+        grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
+        grads.index_add_(0, index, im * scale[:, None])
+        return e[:b], grads.t()[:b]
+
+    def parameter_shift(self, params, indices: Optional[Sequence[int]] = None) -> torch.Tensor:
+        """Gradient by the two-term shift rule (exact for exp(-i theta G / 2), G^2 = I),
+        one pair of batched forward runs per parameter occurrence."""
+        p, b, bp = self._prepare(params)
+        idx = list(range(self.circuit.num_params)) if indices is None else list(indices)
+        grads = torch.zeros(b, len(idx), dtype=torch.float64, device=self.dev)
+        for col, k in enumerate(idx):
+            occ = [i for i in self._param_entries if self.circuit.entries[i].index == k]
+            for entry in occ:
+                sc = self.circuit.entries[entry].scale
+                for sign in (+1, -1):
+                    ops = self._shifted_ops(p, entry, sign * np.pi / 2)
+                    nbits = self.n + (bp.bit_length() - 1)
+                    psi = self._zero_states(bp)
+                    self._run(psi, nbits, ops)
+                    _, e = self._energy(psi, nbits, bp)
+                    grads[:, col] += sign * 0.5 * sc * e[:b]
+        return grads
+
+    def _shifted_ops(self, p: np.ndarray, entry: int, shift: float) -> List[Op]:
+        ops = []
+        for i, op in self._gate_ops(p, False):
+            if i == entry:
+                ent = self.circuit.entries[i]
+                kind, tab = _batched_rotations(ent.kind, ent.scale * p[:, ent.index] + shift)
+                op = Op(op.kind, op.tbits, (), op.mat, tag=op.tag, batch=tab)
+            ops.append(op)
+        return ops
+
+
+class _ExpectationFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, params, engine):
+        e, g = engine.gradient(params)
+        g = g.to(params.device)
+        ctx.save_for_backward(g)
+        return e.to(device=params.device, dtype=params.dtype if params.is_floating_point() else torch.float64)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (g,) = ctx.saved_tensors
+        return (grad_out.to(g.dtype)[:, None] * g).to(grad_out.dtype), None
+
+
+def expectation(params: torch.Tensor, engine: BatchedAdjoint) -> torch.Tensor:
+    """Differentiable batch of energies: torch autograd calls the adjoint sweep
+    (computed together with the forward pass)."""
+    if params.dim() == 1:
+        return _ExpectationFn.apply(params[None, :], engine)[0]
+    return _ExpectationFn.apply(params, engine)

@@ -1,0 +1,208 @@
+"""Drop-in DensityMatrixSimulator
+(QuICT/simulation/density_matrix/density_matrix_simulator.py:14-240).
+
+The reference multiplies dense 2^n x 2^n matrices (M rho M^dagger, and
+sum_i K_i rho K_i^dagger with an O(4^n) embedding per Kraus operator).  Here
+rho is a 2n-bit vector (index = row * 2^n + col, so qubit q is row bit
+(n-1-q)+n and column bit n-1-q) and every operation is a local update on it,
+run by the same fused-pass kernels as the state-vector simulator:
+
+  unitary U on qubits Q   ->  U on the row bits of Q, conj(U) on the column bits
+  Kraus set {K_i} on Q    ->  one superoperator S = sum_i K_i (x) conj(K_i)
+                              acting on (row bits of Q, column bits of Q)
+  measurement             ->  P(0) from the diagonal, then a diagonal projector
+
+A 2-qubit noisy gate is one 16x16 superoperator: one HBM pass at most, instead
+of 2 * |Kraus| dense GEMMs.
+"""
+from __future__ import annotations
+
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from .engine import Engine, require_cuda
+from .fusion import _full_matrix
+from .lowering import Op, classify, lower_gate
+from .state_vector import StateArray
+
+
+def _is_noise_gate(g) -> bool:
+    return hasattr(g, "noise_matrix")
+
+
+def superop(kraus: List[np.ndarray]) -> np.ndarray:
+    """S = sum_i K_i (x) conj(K_i): (S vec(rho))[(r, c)] = sum K rho K^dagger."""
+    k0 = np.asarray(kraus[0], dtype=np.complex128)
+    s = np.zeros((k0.shape[0] ** 2,) * 2, dtype=np.complex128)
+    for k in kraus:
+        k = np.asarray(k, dtype=np.complex128)
+        s += np.kron(k, np.conj(k))
+    return s
+
+
+def lower_dm(g, n: int, legacy_2q_order: bool = False) -> List[Op]:
+    """Gate or NoiseGate -> ops on the 2n-bit vector of rho."""
+    if _is_noise_gate(g):
+        args = list(g.targs)
+        rows = tuple(2 * n - 1 - q for q in args)
+        cols = tuple(n - 1 - q for q in args)
+        s = superop(g.noise_matrix)
+        kind = classify(s)
+        if kind == "diag":
+            return [Op("diag", rows + cols, (), np.diag(s).copy())]
+        return [Op(kind, rows + cols, (), s)]
+    out = []
+    for op in lower_gate(g, n, legacy_2q_order):
+        if op.kind in ("measure", "reset", "perm"):
+            out.append(op)
+            continue
+        row = Op(op.kind, tuple(b + n for b in op.tbits), tuple(b + n for b in op.cbits), op.mat)
+        col = Op(op.kind, op.tbits, op.cbits, np.conj(op.mat))
+        out += [row, col]
+    return out
+
+
+class DensityMatrixSimulator:
+    def __init__(self, device: str = "GPU", precision: str = "double", accumulated_mode: bool = False, *,
+                 gpu_device_id: int = 0, fusion: bool = True, tile_bits: Optional[int] = None,
+                 low_bits: Optional[int] = None, merge_bits: int = 2, seed=None):
+        if device != "GPU":
+            raise ValueError(f"DensityMatrixSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
+        if precision not in ("single", "double"):
+            raise ValueError("DensityMatrixSimulator.precision must be 'single' or 'double'")
+        self._precision = np.complex128 if precision == "double" else np.complex64
+        self._tdtype = torch.complex128 if precision == "double" else torch.complex64
+        self._accumulated_mode = accumulated_mode
+        self._tdev = require_cuda(gpu_device_id)
+        self._engine = Engine(self._tdev, fusion=fusion, tile_bits=tile_bits, low_bits=low_bits,
+                              merge_bits=merge_bits)
+        self._rng = seed if hasattr(seed, "random") else np.random.default_rng(seed)
+        self._density_matrix: Optional[torch.Tensor] = None
+        self._circuit = None
+        self._origin_circuit = None
+        self._noise_model = None
+        self._qubits = 0
+        self.last_sample_indices: Optional[torch.Tensor] = None
+
+    @property
+    def engine(self) -> Engine:
+        return self._engine
+
+    @property
+    def density_matrix(self) -> StateArray:
+        return StateArray(self._density_matrix)
+
+    @property
+    def _qs_dtype(self) -> int:
+        return N.QS_C128 if self._precision == np.complex128 else N.QS_C64
+
+    # ---- reference surface ---------------------------------------------------------------
+    def initial_circuit(self, circuit, noise_model=None):
+        self._origin_circuit = circuit
+        self._noise_model = noise_model
+        self._circuit = circuit if noise_model is None else noise_model.transpile(circuit, self._accumulated_mode)
+        self._qubits = int(circuit.width())
+
+    def initial_density_matrix(self, qubits: int):
+        self._density_matrix = torch.empty((1 << qubits, 1 << qubits), dtype=self._tdtype, device=self._tdev)
+        N.call("qs_init_zero", self._density_matrix.data_ptr(), 2 * qubits, self._qs_dtype, self._engine.stream)
+
+    @staticmethod
+    def check_matrix(matrix) -> bool:
+        """Hermitian, positive semi-definite, unit trace (density_matrix_simulator.py:62-80)."""
+        m = np.asarray(matrix)
+        if not np.allclose(m.T.conjugate(), m):
+            raise ValueError("The conjugate transpose of density matrix do not equal to itself.")
+        ev = np.linalg.eigvalsh(m)
+        if np.any((ev < 0) & ~np.isclose(ev, 0, rtol=1e-4, atol=1e-8)):
+            raise ValueError("The eigenvalues of density matrix should be non-negative")
+        if not np.isclose(np.trace(m), 1, rtol=1e-4):
+            raise ValueError("The sum of trace of density matrix should be 1.")
+        return True
+
+    def run(self, circuit, density_matrix=None, noise_model=None, use_previous: bool = False) -> StateArray:
+        self.initial_circuit(circuit, noise_model)
+        n = self._qubits
+        if density_matrix is not None:
+            dm = density_matrix.tensor if isinstance(density_matrix, StateArray) else density_matrix
+            if isinstance(dm, torch.Tensor):
+                self.check_matrix(dm.detach().cpu().numpy())
+                self._density_matrix = dm.to(device=self._tdev, dtype=self._tdtype).contiguous().clone()
+            else:
+                self.check_matrix(dm)
+                self._density_matrix = torch.from_numpy(np.ascontiguousarray(dm, dtype=self._precision)).to(self._tdev)
+            if tuple(self._density_matrix.shape) != (1 << n, 1 << n):
+                raise ValueError("density matrix shape does not match the circuit")
+        elif self._density_matrix is None or not use_previous or self._density_matrix.shape[0] != (1 << n):
+            self.initial_density_matrix(n)
+        self._run(self._circuit)
+        if noise_model is not None and hasattr(noise_model, "apply_readout_error"):
+            noise_model.apply_readout_error(circuit.qubits)
+        torch.cuda.synchronize(self._tdev)
+        return self.density_matrix
+
+    def _run(self, circuit):
+        n = self._qubits
+        vec = self._density_matrix.view(-1)
+        pending: List[Op] = []
+        for g in circuit.gates:
+            for op in lower_dm(g, n):
+                if op.kind == "measure":
+                    self._engine.apply_ops(vec, 2 * n, pending)
+                    pending = []
+                    self.apply_measure(op.qubit)
+                elif op.kind in ("reset", "perm"):
+                    raise TypeError(f"DensityMatrixSimulator does not support {op.kind} gates")
+                else:
+                    pending.append(op)
+        self._engine.apply_ops(vec, 2 * n, pending)
+
+    def apply_measure(self, qubit: int, u: Optional[float] = None) -> int:
+        """Reference rule (density_matrix_simulator.py:182-208): P(0) = trace of the
+        projected diagonal; outcome 1 iff u > P(0); rho <- P rho P / p."""
+        n = self._qubits
+        b = n - 1 - qubit
+        p0 = self._engine.prob0(self._density_matrix, n, b, N.QS_SRC_DM)
+        if u is None:
+            u = float(self._rng.random())
+        one = u > p0
+        p = (1.0 - p0) if one else p0
+        d = np.zeros(4, dtype=np.complex128)
+        d[3 if one else 0] = 1.0 / p
+        self._engine.apply_ops(self._density_matrix.view(-1), 2 * n, [Op("diag", (b + n, b), (), d)])
+        if self._circuit is not None:
+            self._circuit.qubits[qubit].measured = int(one)
+        if self._origin_circuit is not None and self._origin_circuit is not self._circuit:
+            self._origin_circuit.qubits[qubit].measured = int(one)
+        return int(one)
+
+    def sample(self, shots: int, uniforms=None, mode: str = "cdf", seed=None):
+        """Counts (length 2^n) of `shots` full-register measurements drawn from
+        diag(rho); same rules as StateVectorSimulator.sample.  Readout errors of
+        the noise model are applied to every shot, as the reference does."""
+        if self._density_matrix is None:
+            raise RuntimeError("DensityMatrixSimulator sample without run any circuit.")
+        n = self._qubits
+        m = N.QS_SAMPLE_CDF if mode == "cdf" else N.QS_SAMPLE_SEQ
+        per = 1 if m == N.QS_SAMPLE_CDF else n
+        if uniforms is None:
+            rng = np.random.default_rng(seed) if seed is not None else self._rng
+            uniforms = rng.random(shots * per)
+        u = torch.as_tensor(np.asarray(uniforms, dtype=np.float64).ravel()[: shots * per])
+        idx = self._engine.sample_indices(self._density_matrix, n, u, m, N.QS_SRC_DM)
+        self.last_sample_indices = idx
+        nm = self._noise_model
+        if nm is not None and getattr(nm, "_readout_errors", None):
+            host = idx.cpu().numpy()
+            counts = np.zeros(1 << n, dtype=np.int64)
+            qs = self._circuit.qubits
+            for v in host:
+                for q in range(n):
+                    qs[q].measured = (int(v) >> (n - 1 - q)) & 1
+                nm.apply_readout_error(qs)
+                counts[int(qs)] += 1
+            return counts.tolist()
+        return self._engine.histogram(idx, 1 << n).cpu().numpy().tolist()

@@ -47,6 +47,8 @@ Step = Union[Pass, Single]
 
 
 def fusable(op: Op) -> bool:
+    if op.kind == "expect":
+        return op.m <= 2 or op.is_diag_expect
     return op.kind in ("mat", "diag", "antidiag", "swap") and op.m <= MAX_FUSED_M
 
 
@@ -219,7 +221,9 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2) -> List[Op]
 
 def op_entries(op: Op) -> int:
     """Matrix entries the op occupies in a pass's on-chip matrix table."""
-    return (1 << op.m) if op.kind == "diag" else (1 << (2 * op.m))
+    if op.kind == "diag" or (op.kind == "expect" and op.is_diag_expect):
+        return 1 << op.m
+    return 1 << (2 * op.m)
 
 
 def op_cost(op: Op) -> float:
@@ -252,14 +256,24 @@ class MatrixTable:
             self.size += a.size
         return off
 
+    def add_block(self, block: np.ndarray) -> int:
+        """Append a per-instance block (instances x entries) without de-duplication."""
+        a = np.ascontiguousarray(block, dtype=np.complex128).ravel()
+        off = self.size
+        self._chunks.append(a)
+        self.size += a.size
+        return off
+
     def array(self) -> np.ndarray:
         if not self._chunks:
             return np.zeros(1, dtype=np.complex128)
         return np.concatenate(self._chunks)
 
 
-def emit(passes: Sequence[Pass], table: MatrixTable):
-    """Convert passes into ctypes (qs_pass[], qs_op[]) arrays, filling `table`."""
+def emit(passes: Sequence[Pass], table: MatrixTable, inst_shift: int = 0):
+    """Convert passes into ctypes (qs_pass[], qs_op[]) arrays, filling `table`.
+    inst_shift > 0 marks a batched state (instance = index >> inst_shift); ops
+    with per-instance tables (``Op.batch``) then get a matrix stride."""
     cps = (N.qs_pass * max(1, len(passes)))()
     nops = sum(len(p.ops) for p in passes)
     cops = (N.qs_op * max(1, nops))()
@@ -270,6 +284,7 @@ def emit(passes: Sequence[Pass], table: MatrixTable):
         for j, h in enumerate(p.hi):
             cp.hi[j] = h
         cp.op_begin, cp.op_count = o, len(p.ops)
+        cp.inst_shift = inst_shift
         local = {b: b for b in range(p.nlow)}
         for j, h in enumerate(p.hi):
             local[h] = p.nlow + j
@@ -291,7 +306,20 @@ def emit(passes: Sequence[Pass], table: MatrixTable):
                     gc |= 1 << b
             c.lctrl, c.gctrl = lc, gc
             c.flags = 0
-            if op.kind == "diag":
+            if op.batch is not None:
+                c.kind = {"mat": N.QS_OP_MAT, "diag": N.QS_OP_DIAG, "antidiag": N.QS_OP_ANTI,
+                          "swap": N.QS_OP_SWAP}[op.kind]
+                c.mat = table.add_block(op.batch)
+                c.mat_stride = op.batch.shape[1]
+            elif op.kind == "expect":
+                c.kind = N.QS_OP_EXPECT
+                c.slot = op.slot
+                if op.is_diag_expect:
+                    c.flags = N.QS_OPF_DIAG
+                    c.mat = table.add(np.diag(op.mat))
+                else:
+                    c.mat = table.add(op.mat)
+            elif op.kind == "diag":
                 c.kind = N.QS_OP_DIAG
                 c.mat = table.add(op.mat)
             else:

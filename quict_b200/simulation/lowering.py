@@ -33,22 +33,30 @@ class Op:
     mat: Optional[np.ndarray] = None  # complex128: mat (2^m,2^m), diag (2^m,), antidiag (2,2), swap (4,4)
     perm: Optional[Tuple[int, ...]] = None  # "perm": source qubit of each destination qubit
     qubit: Optional[int] = None   # measure / reset: circuit qubit index
-    tag: object = None            # caller data (e.g. parameter index for gradients)
+    tag: object = None            # caller data (e.g. parameter index for gradients); blocks merging
+    batch: Optional[np.ndarray] = None  # per-instance tables, shape (instances, entries)
+    slot: int = -1                # "expect": output slot
 
     @property
     def m(self) -> int:
         return len(self.tbits)
 
     @property
+    def is_diag_expect(self) -> bool:
+        return self.kind == "expect" and classify(self.mat) == "diag"
+
+    @property
     def xbits(self) -> frozenset:
         """Bits on which the op is not diagonal (must be tile-resident when fused)."""
-        return frozenset(self.tbits) if self.kind in ("mat", "antidiag", "swap") else frozenset()
+        if self.kind in ("mat", "antidiag", "swap") or (self.kind == "expect" and not self.is_diag_expect):
+            return frozenset(self.tbits)
+        return frozenset()
 
     @property
     def zbits(self) -> frozenset:
         """Bits on which the op is block-diagonal (controls, diagonal targets)."""
         z = set(self.cbits)
-        if self.kind == "diag":
+        if self.kind == "diag" or self.is_diag_expect:
             z |= set(self.tbits)
         return frozenset(z)
 

@@ -280,6 +280,80 @@ def main():
         out[f"n{n}_kraus1"] = np.array([np.asarray(k) for k in e1.kraus])
         out[f"n{n}_kraus2"] = np.array([np.asarray(k) for k in e2.kraus])
     np.savez_compressed(os.path.join(HERE, "dm.npz"), **out)
+
+    # ---- energies and parameter-shift gradients from reference amplitudes --------------------
+    # hardware-efficient ansatz: layers of Ry, Rz on every qubit + CZ ring;
+    # H = sum Z_i Z_{i+1} + 0.5 sum X_i (open chain).  QAOA MaxCut: H on all,
+    # p layers of Rzz(-gamma) per edge and Rx(2 beta) per qubit; C = sum (1 - ZZ)/2.
+    out = {}
+    X = np.array([[0, 1], [1, 0]])
+    Z = np.diag([1.0, -1.0])
+
+    def op_on(n, ps):
+        m = np.eye(1)
+        for q in range(n):
+            m = np.kron(m, ps.get(q, np.eye(2)))
+        return m
+
+    def hea_gates(n, layers, th):
+        gl, p = [], 0
+        for _ in range(layers):
+            for q in range(n):
+                gl.append(["ry", [q], [float(th[p])]]); p += 1
+            for q in range(n):
+                gl.append(["rz", [q], [float(th[p])]]); p += 1
+            for q in range(n - 1):
+                gl.append(["cz", [q, q + 1], []])
+            gl.append(["cz", [n - 1, 0], []])
+        return gl
+
+    def energy(gl, n, h):
+        v = sv_cpu(build(gl, n))
+        return float(np.real(np.vdot(v, h @ v)))
+
+    n, layers = 4, 2
+    h = sum(op_on(n, {q: Z, q + 1: Z}) for q in range(n - 1)) + 0.5 * sum(op_on(n, {q: X}) for q in range(n))
+    rng = np.random.default_rng(501)
+    th = rng.uniform(0, 2 * np.pi, 2 * n * layers)
+    g = np.zeros_like(th)
+    for k in range(th.size):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += np.pi / 2
+        tm[k] -= np.pi / 2
+        g[k] = 0.5 * (energy(hea_gates(n, layers, tp), n, h) - energy(hea_gates(n, layers, tm), n, h))
+    out["hea_params"], out["hea_energy"], out["hea_grad"] = th, energy(hea_gates(n, layers, th), n, h), g
+
+    n, p = 6, 2
+    edges = [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 0), (0, 3), (1, 4), (2, 5)]
+    cost = sum(0.5 * (np.eye(1 << n) - op_on(n, {a: Z, b: Z})) for a, b in edges)
+
+    def qaoa_gates(gb):
+        gl = [["h", [q], []] for q in range(n)]
+        for layer in range(p):
+            for a, b in edges:
+                gl.append(["rzz", [a, b], [float(-gb[layer])]])
+            for q in range(n):
+                gl.append(["rx", [q], [float(2 * gb[p + layer])]])
+        return gl
+
+    gb = rng.uniform(0, np.pi, 2 * p)
+    # per-occurrence shift rule: gamma_l appears in |E| gates with scale -1, beta_l in n gates with scale 2
+    gq = np.zeros(2 * p)
+    for layer in range(p):
+        for which, scale, count in ((layer, -1.0, len(edges)), (p + layer, 2.0, n)):
+            for occ in range(count):
+                for sign in (1, -1):
+                    gl = qaoa_gates(gb)
+                    # locate the occ-th gate of this parameter and shift its angle by +-pi/2
+                    pos = [i for i, (nm, _, _) in enumerate(gl) if (nm == "rzz" and which == layer
+                           and i >= n + layer * (len(edges) + n) and i < n + layer * (len(edges) + n) + len(edges))
+                           or (nm == "rx" and which == p + layer and i >= n + layer * (len(edges) + n) + len(edges)
+                               and i < n + (layer + 1) * (len(edges) + n))][occ]
+                    gl[pos][2] = [gl[pos][2][0] + sign * np.pi / 2]
+                    gq[which] += sign * 0.5 * scale * energy(gl, n, cost)
+    out["qaoa_edges"], out["qaoa_params"] = np.array(edges), gb
+    out["qaoa_energy"], out["qaoa_grad"] = energy(qaoa_gates(gb), n, cost), gq
+    np.savez_compressed(os.path.join(HERE, "grad.npz"), **out)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,151 @@
+"""Density-matrix simulator: CPU checks of the superoperator lowering and the
+noise model, GPU parity against the reference fixtures and the FP64 oracle
+(complex128 within 1e-12, complex64 within 1e-5)."""
+import json
+
+import numpy as np
+import pytest
+
+from conftest import build_circuit, golden, oracle_gates
+from oracle import dm as odm
+from oracle import sv as osv
+
+
+def _noise_model(gates_1q, gates_2q, gamma=5e-3, p1=1e-3, p2=1e-2):
+    from quict_b200.core import NoiseModel, DampingError, DepolarizingError
+    amp = DampingError(amplitude_prob=gamma, phase_prob=0)
+    nm = NoiseModel(basic_gates=gates_1q + gates_2q)
+    nm.add_noise_for_all_qubits(amp.compose(DepolarizingError(p1, 1)), gates_1q)
+    nm.add_noise_for_all_qubits(amp.tensor(amp).compose(DepolarizingError(p2, 2)), gates_2q)
+    return nm
+
+
+def _apply_dm_ops(rho, n, ops):
+    v = rho.reshape(-1).astype(np.complex128)
+    for op in ops:
+        bits = list(op.cbits) + list(op.tbits)
+        u = op.dense()
+        if op.cbits:
+            d = u.shape[0] << len(op.cbits)
+            f = np.eye(d, dtype=np.complex128)
+            f[-u.shape[0]:, -u.shape[0]:] = u
+            u = f
+        v = osv.apply_matrix(v, 2 * n, u, [2 * n - 1 - b for b in bits])
+    return v.reshape(1 << n, 1 << n)
+
+
+@pytest.mark.parametrize("n", [3, 4])
+def test_dm_lowering_matches_reference_fixture(n):
+    from quict_b200.simulation.density_matrix import lower_dm
+    d = golden("dm.npz")
+    gl = json.loads(str(d[f"n{n}_gates"]))
+    c = build_circuit(gl, n)
+    nm = _noise_model(["h", "u3", "rx"], ["rzz", "swap", "cx", "cz"])
+    noisy = nm.transpile(c, accumulated_mode=True)
+    ops = [op for g in noisy.gates for op in lower_dm(g, n)]
+    rho = _apply_dm_ops(odm.zero_dm(n), n, ops)
+    np.testing.assert_allclose(rho, d[f"n{n}_noisy"], rtol=0, atol=1e-12)
+    clean = [op for g in c.gates for op in lower_dm(g, n)]
+    np.testing.assert_allclose(_apply_dm_ops(odm.zero_dm(n), n, clean), d[f"n{n}_clean"], rtol=0, atol=1e-12)
+
+
+def test_transpile_attaches_one_noise_gate_per_matched_gate():
+    from quict_b200.core import Circuit, H, CX, Rz
+    nm = _noise_model(["h"], ["cx"])
+    c = Circuit(3)
+    H | c(0)
+    CX | c([0, 1])
+    Rz(0.3) | c(2)
+    t = nm.transpile(c, accumulated_mode=True)
+    kinds = [getattr(g, "type", None) for g in t.gates]
+    assert kinds[0] == "noise" and kinds[1] == "noise" and kinds[2].name == "rz"
+    assert len(t.gates[0].noise_matrix) == 8 and len(t.gates[1].noise_matrix) == 64
+
+
+def test_readout_error_is_a_confusion_row_draw():
+    from quict_b200.core import ReadoutError, Circuit
+    err = ReadoutError([[0.0, 1.0], [1.0, 0.0]])  # always flips
+    from quict_b200.core import NoiseModel
+    nm = NoiseModel()
+    nm.add_readout_error(err, [0, 2])
+    c = Circuit(3)
+    for q, v in enumerate([0, 1, 1]):
+        c.qubits[q].measured = v
+    nm.apply_readout_error(c.qubits)
+    assert [q.measured for q in c.qubits] == [1, 1, 0]
+
+
+# ------------------------------------------------------------------ GPU parity
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [3, 4])
+@pytest.mark.parametrize("fusion", [True, False])
+def test_dm_gpu_matches_reference_fixture(cuda_ok, n, fusion):
+    from quict_b200.simulation import DensityMatrixSimulator
+    d = golden("dm.npz")
+    gl = json.loads(str(d[f"n{n}_gates"]))
+    nm = _noise_model(["h", "u3", "rx"], ["rzz", "swap", "cx", "cz"])
+    sim = DensityMatrixSimulator("GPU", accumulated_mode=True, fusion=fusion)
+    rho = sim.run(build_circuit(gl, n), noise_model=nm).get()
+    np.testing.assert_allclose(rho, d[f"n{n}_noisy"], rtol=0, atol=1e-12)
+    rho = DensityMatrixSimulator("GPU", fusion=fusion).run(build_circuit(gl, n)).get()
+    np.testing.assert_allclose(rho, d[f"n{n}_clean"], rtol=0, atol=1e-12)
+    sim = DensityMatrixSimulator("GPU", "single", accumulated_mode=True, fusion=fusion)
+    rho = sim.run(build_circuit(gl, n), noise_model=nm).get()
+    np.testing.assert_allclose(rho, d[f"n{n}_noisy"], rtol=0, atol=1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [7, 12])
+def test_dm_config2_style_vs_oracle(cuda_ok, n):
+    """150-gate config-0 gate set with composed damping+depolarizing per gate."""
+    from quict_b200.core import Circuit
+    from quict_b200.simulation import DensityMatrixSimulator
+    size = 150 if n == 7 else 12
+    c = Circuit(n)
+    c.random_append(size, seed=n)
+    one = ["h", "x", "rx", "ry", "rz", "u3"]
+    two = ["cx", "cz", "rzz", "swap"]
+    nm = _noise_model(one, two)
+    rho = DensityMatrixSimulator("GPU", accumulated_mode=True).run(c, noise_model=nm).get()
+    k1, k2 = odm.composed_noise_1q(5e-3, 1e-3), odm.composed_noise_2q(5e-3, 1e-2)
+    ref = odm.run(oracle_gates(c), n, noise=lambda a: k1 if len(a) == 1 else k2)
+    np.testing.assert_allclose(rho, ref, rtol=0, atol=1e-12)
+    assert abs(np.trace(rho) - 1) < 1e-12
+
+
+@pytest.mark.gpu
+def test_dm_measure_and_sample(cuda_ok):
+    from quict_b200.core import Circuit, H, CX, Measure
+    from quict_b200.simulation import DensityMatrixSimulator
+    n = 4
+    c = Circuit(n)
+    H | c(0)
+    for q in range(n - 1):
+        CX | c([q, q + 1])
+    sim = DensityMatrixSimulator("GPU", seed=11)
+    rho = sim.run(c).get()
+    counts = sim.sample(2000, seed=5)
+    assert counts[0] + counts[-1] == 2000 and counts[0] > 800 and counts[-1] > 800
+    # sequential rule with explicit uniforms equals the oracle's per-qubit rule
+    u = np.random.default_rng(3).random(64 * n)
+    sim.sample(64, uniforms=u, mode="sequential")
+    got = sim.last_sample_indices.cpu().numpy()
+    probs = np.real(np.diag(rho))
+    want = osv.sample_sequential_fast(np.sqrt(probs).astype(np.complex128), n, u)
+    np.testing.assert_array_equal(got, want)
+    # mid-circuit measurement: collapse matches the oracle projector
+    c2 = Circuit(n)
+    H | c2(0)
+    CX | c2([0, 1])
+    Measure | c2(1)
+    sim2 = DensityMatrixSimulator("GPU", seed=type("U", (), {"random": staticmethod(lambda: 0.7)})())
+    rho2 = sim2.run(c2).get()
+    r = odm.run(oracle_gates_unitary(c2), n)
+    r, b = odm.measure(r, n, 1, 0.7)
+    np.testing.assert_allclose(rho2, r, atol=1e-12)
+    assert c2.qubits[1].measured == b
+
+
+def oracle_gates_unitary(c):
+    return [(np.asarray(g.matrix, dtype=np.complex128), list(g.cargs) + list(g.targs))
+            for g in c.gates if g.type.name not in ("measure",)]

@@ -1,0 +1,144 @@
+"""Batched energies and adjoint gradients.
+
+Pins: tests/golden/grad.npz holds energies and parameter-shift gradients
+computed from the REFERENCE StateVectorSimulator's amplitudes.  Tolerances:
+complex128 energies / gradients within 1e-10, complex64 within 1e-4 of the
+FP64 oracle (the north_star's gradient bound)."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import observe as oobs
+from oracle import sv as osv
+
+
+def _hea(n, layers):
+    from quict_b200.differentiation import hardware_efficient_ansatz, ising_observable
+    return hardware_efficient_ansatz(n, layers), ising_observable(n)
+
+
+def _matrices_fn(circ):
+    from quict_b200.differentiation import rotation
+
+    def fn(params, shifts):
+        out = []
+        for i, e in enumerate(circ.entries):
+            if e.kind == "fixed":
+                out.append((e.matrix, list(e.qubits)))
+            else:
+                out.append((rotation(e.kind, e.scale * params[e.index] + shifts.get(i, 0.0)), list(e.qubits)))
+        return out
+    return fn
+
+
+def _occurrences(circ):
+    return [(e.index, i, e.scale) for i, e in enumerate(circ.entries) if e.kind != "fixed"]
+
+
+def test_oracle_gradients_match_reference_fixture():
+    d = golden("grad.npz")
+    circ, obs = _hea(4, 2)
+    fn = _matrices_fn(circ)
+    h = obs.matrix()
+    th = d["hea_params"]
+    assert abs(oobs.energy(fn(th, {}), 4, h) - float(d["hea_energy"])) < 1e-12
+    np.testing.assert_allclose(oobs.param_shift(fn, th, 4, h, _occurrences(circ)), d["hea_grad"], atol=1e-12)
+    np.testing.assert_allclose(oobs.finite_diff(fn, th, 4, h), d["hea_grad"], atol=1e-8)
+    from quict_b200.differentiation import qaoa_circuit, maxcut_observable
+    edges = [tuple(e) for e in d["qaoa_edges"]]
+    qc = qaoa_circuit(6, edges, 2)
+    fq = _matrices_fn(qc)
+    hq = maxcut_observable(6, edges).matrix()
+    gb = d["qaoa_params"]
+    assert abs(oobs.energy(fq(gb, {}), 6, hq) - float(d["qaoa_energy"])) < 1e-12
+    np.testing.assert_allclose(oobs.param_shift(fq, gb, 6, hq, _occurrences(qc)), d["qaoa_grad"], atol=1e-11)
+
+
+def test_pauli_masks_and_dense_matrix_agree():
+    from quict_b200.differentiation import PauliSum
+    hs = PauliSum(3).add(0.7, {0: "X", 2: "Y"}).add(-1.1, {1: "Z"}).add(0.25, {})
+    x, z, c = hs.masks()
+    v = np.random.default_rng(0).normal(size=8) + 1j * np.random.default_rng(1).normal(size=8)
+    out = np.zeros(8, dtype=np.complex128)
+    for t in range(len(x)):
+        coeff = complex(c[2 * t], c[2 * t + 1]) * (1j ** bin(int(x[t]) & int(z[t])).count("1"))
+        for j in range(8):
+            src = j ^ int(x[t])
+            out[j] += coeff * (-1) ** bin(int(z[t]) & src).count("1") * v[src]
+    np.testing.assert_allclose(out, hs.matrix() @ v, atol=1e-14)
+
+
+def test_random_regular_graph_is_regular():
+    from quict_b200.differentiation import random_regular_graph
+    for n in (10, 16, 24):
+        es = random_regular_graph(n, 3, np.random.default_rng(n))
+        deg = np.bincount(np.array(es).ravel(), minlength=n)
+        assert len(es) == 3 * n // 2 and np.all(deg == 3)
+
+
+# ------------------------------------------------------------------ GPU
+pytestmark_gpu = pytest.mark.gpu
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("double", 1e-10), ("single", 1e-4)])
+def test_adjoint_matches_reference_fixture(cuda_ok, precision, tol):
+    from quict_b200.differentiation import BatchedAdjoint
+    d = golden("grad.npz")
+    circ, obs = _hea(4, 2)
+    eng = BatchedAdjoint(circ, obs, precision)
+    e, g = eng.gradient(d["hea_params"][None, :])
+    assert abs(float(e[0]) - float(d["hea_energy"])) < tol
+    np.testing.assert_allclose(g[0].cpu().numpy(), d["hea_grad"], atol=tol)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("double", 1e-10), ("single", 1e-4)])
+def test_adjoint_qaoa_matches_reference_fixture(cuda_ok, precision, tol):
+    from quict_b200.differentiation import BatchedAdjoint, qaoa_circuit, maxcut_observable
+    d = golden("grad.npz")
+    edges = [tuple(int(a) for a in e) for e in d["qaoa_edges"]]
+    eng = BatchedAdjoint(qaoa_circuit(6, edges, 2), maxcut_observable(6, edges), precision)
+    e, g = eng.gradient(d["qaoa_params"][None, :])
+    assert abs(float(e[0]) - float(d["qaoa_energy"])) < tol * 10
+    np.testing.assert_allclose(g[0].cpu().numpy(), d["qaoa_grad"], atol=tol * 10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,layers,batch", [(6, 2, 5), (13, 2, 4), (16, 1, 3)])
+def test_batched_adjoint_vs_oracle(cuda_ok, n, layers, batch):
+    from quict_b200.differentiation import BatchedAdjoint
+    circ, obs = _hea(n, layers)
+    rng = np.random.default_rng(n)
+    params = rng.uniform(0, 2 * np.pi, (batch, circ.num_params))
+    fn = _matrices_fn(circ)
+    h = obs.matrix() if n <= 10 else None
+    for precision, tol in (("double", 1e-10), ("single", 1e-4)):
+        eng = BatchedAdjoint(circ, obs, precision)
+        e, g = eng.gradient(params)
+        states = eng.states(params).cpu().numpy()
+        for b in range(batch):
+            psi = osv.run(fn(params[b], {}), n)
+            np.testing.assert_allclose(states[b], psi, atol=10 * tol)
+            if h is not None:
+                assert abs(float(e[b]) - oobs.energy(fn(params[b], {}), n, h)) < tol
+        if h is not None:
+            for b in range(min(batch, 2)):
+                want = oobs.param_shift(fn, params[b], n, h, _occurrences(circ))
+                np.testing.assert_allclose(g[b].cpu().numpy(), want, atol=tol)
+        # GPU parameter shift agrees with the adjoint sweep (same GPU kernels)
+        ps = eng.parameter_shift(params, indices=[0, 1, circ.num_params - 1])
+        np.testing.assert_allclose(ps.cpu().numpy(), g[:, [0, 1, circ.num_params - 1]].cpu().numpy(), atol=tol)
+
+
+@pytest.mark.gpu
+def test_autograd_function(cuda_ok):
+    import torch
+    from quict_b200.differentiation import BatchedAdjoint, expectation
+    circ, obs = _hea(5, 2)
+    eng = BatchedAdjoint(circ, obs, "double")
+    p = torch.tensor(np.random.default_rng(3).uniform(0, 6, (3, circ.num_params)), requires_grad=True)
+    e = expectation(p, eng)
+    e.sum().backward()
+    _, g = eng.gradient(p.detach())
+    np.testing.assert_allclose(p.grad.numpy(), g.cpu().numpy(), atol=1e-12)
