@@ -213,6 +213,25 @@ int qs_sample_prepare(const void* src, int n, int dtype, int src_kind,
 int qs_sample(const void* src, int n, int dtype, int src_kind, const void* ws,
               size_t ws_bytes, const double* u_dev, int64_t shots, int mode,
               int64_t* out_idx_dev, void* stream);
+/* Allocation-free variant of qs_sample_prepare + qs_sample.  No counterpart
+ * in the reference.  It exists for callers that cannot allocate device
+ * memory: a process whose device memory is already handed out to its own
+ * pool allocator (so an extra cudaMalloc can fail or fragment it), or a
+ * C / FFI caller that owns only the state, the uniforms and the output and
+ * has nowhere to keep a workspace.  The FP64 sum tree lives in a file-scope
+ * device array of the library (1 MiB on every device that loads it, held until
+ * the process exits), so the call allocates nothing and frees nothing.
+ * Limit: n <= QS_NOALLOC_SAMPLE_MAX_QUBITS (26); larger n returns QS_EINVAL.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture begins.  All calls share the one array and it
+ * keeps the last call's contents (each call overwrites every node it reads),
+ * so calls whose work overlaps on the GPU -- e.g. on two streams -- race:
+ * order them on one stream.  Arguments and results as qs_sample. */
+#define QS_NOALLOC_SAMPLE_MAX_QUBITS 26
+int qs_sample_noalloc(const void* src, int n, int dtype, int src_kind, const double* u_dev,
+                      int64_t shots, int mode, int64_t* out_idx_dev, void* stream);
+
 /* counts_dev[idx_dev[s]] += 1 (int64, caller zeroes counts_dev). */
 int qs_histogram(const int64_t* idx_dev, int64_t shots, int64_t* counts_dev,
                  int64_t ncounts, void* stream);

@@ -101,6 +101,7 @@ SIGNATURES = {
     "qs_sample_prepare": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp]),
     "qs_sample": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp, _i64, _i, _vp, _vp]),
     "qs_histogram": (_i, [_vp, _i64, _vp, _i64, _vp]),
+    "qs_sample_noalloc": (_i, [_vp, _i, _i, _i, _vp, _i64, _i, _vp, _vp]),
 }
 
 _lib = None

@@ -6,6 +6,8 @@
 // 2^B-amplitude blocks at the leaves, a binary heap above them.  Each shot is
 // one warp that walks the heap from the root (qubit 0 = the vector's top bit
 // first) and finishes inside its leaf block from the block's own amplitudes.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace qs {
@@ -380,4 +382,72 @@ extern "C" int qs_histogram(const int64_t* idx_dev, int64_t shots, int64_t* coun
     k_hist<<<grid, 256, 0, as_stream(stream)>>>(idx_dev, shots, (unsigned long long*)counts_dev, ncounts);
     QS_CHECK_LAUNCH("qs_histogram");
     return QS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free sampling.  The sum tree lives in a file-scope device array
+// instead of a caller workspace, for callers that can only hand over the
+// state, the uniforms and the output buffer (see include/qsim.h).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocMaxQubits = QS_NOALLOC_SAMPLE_MAX_QUBITS;
+constexpr size_t kNoAllocTreeDoubles = size_t(2) << (kNoAllocMaxQubits - kBlockBits);  // 1 MiB
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_tree[kNoAllocTreeDoubles];
+
+namespace {
+// Device address of g_noalloc_tree, looked up once per device with that device
+// current (the array's host-side name is not a device address).
+int noalloc_tree_ptr(double** out) {
+    static std::mutex mu;
+    static double* addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("qs_sample_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+        return QS_ECUDA;
+    }
+    QS_REQUIRE(dev >= 0 && dev < 64, "qs_sample_noalloc: device %d outside [0, 64)", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_tree);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error("qs_sample_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return QS_ECUDA;
+        }
+        addr[dev] = static_cast<double*>(p);
+    }
+    *out = addr[dev];
+    return QS_OK;
+}
+}  // namespace
+
+extern "C" int qs_sample_noalloc(const void* src, int n, int dtype, int src_kind, const double* u_dev,
+                                 int64_t shots, int mode, int64_t* out_idx_dev, void* stream) {
+    int rc = check_src(src, n, dtype, src_kind);
+    if (rc) return rc;
+    if (n > kNoAllocMaxQubits) {
+        set_error("qs_sample_noalloc: %d qubits exceed its fixed %d-qubit limit (a %zu-byte static sum tree); "
+                  "use qs_sample_prepare/qs_sample with a workspace",
+                  n, kNoAllocMaxQubits, sizeof(double) * kNoAllocTreeDoubles);
+        return QS_EINVAL;
+    }
+    QS_REQUIRE(mode == QS_SAMPLE_CDF || mode == QS_SAMPLE_SEQ, "bad sample mode %d", mode);
+    QS_REQUIRE(shots >= 0, "negative shot count");
+    QS_REQUIRE(u_dev != nullptr && out_idx_dev != nullptr, "null uniforms or output");
+    if (shots == 0) return QS_OK;
+    double* tree = nullptr;
+    rc = noalloc_tree_ptr(&tree);
+    if (rc) return rc;
+    // every node the descent reads is written by the prepare step, so the
+    // tree needs no clearing between calls
+    cudaStream_t st = as_stream(stream);
+    if (dtype == QS_C128) {
+        rc = prepare_t<double2>(src, n, src_kind, tree, st);
+        return rc ? rc : sample_t<double2>(src, n, src_kind, tree, u_dev, shots, mode, out_idx_dev, st);
+    }
+    rc = prepare_t<float2>(src, n, src_kind, tree, st);
+    return rc ? rc : sample_t<float2>(src, n, src_kind, tree, u_dev, shots, mode, out_idx_dev, st);
 }
