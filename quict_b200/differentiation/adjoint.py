@@ -164,40 +164,82 @@ class BatchedAdjoint:
         _, e = self._energy(psi, nbits, bp)
         return e[:b]
 
-    def gradient(self, params) -> Tuple[torch.Tensor, torch.Tensor]:
-        """(energies (B,), gradients (B, P)) in FP64."""
+    def plan_gradient(self, params) -> "GradientPlan":
+        """Host work for one gradient evaluation: op tables, pass plans, device
+        buffers.  ``launch`` then issues kernels only (so it can be captured in a
+        CUDA graph and replayed)."""
         p, b, bp = self._prepare(params)
         nbits = self.n + (bp.bit_length() - 1)
-        psi = self._zero_states(bp)
-        self._run(psi, nbits, [op for _, op in self._gate_ops(p, False)])
-        lam, e = self._energy(psi, nbits, bp)
-        # backward sweep: EXPECT(G_k) then U_k^dagger, k = L..1
+        gp = GradientPlan(b=b, bp=bp, nbits=nbits)
+        gp.fwd = self._build(nbits, [op for _, op in self._gate_ops(p, False)], adjoint=False)
         inv = self._gate_ops(p, True)
         slot_of = {entry: s for s, entry in enumerate(self._param_entries)}
         ops: List[Op] = []
         for entry, op in reversed(inv):
             ent = self.circuit.entries[entry]
             if ent.kind != "fixed":
-                g = GENERATORS[ent.kind]
-                ops.append(Op("expect", op.tbits, (), g, tag=("expect", entry), slot=slot_of[entry]))
+                ops.append(Op("expect", op.tbits, (), GENERATORS[ent.kind], tag=("expect", entry),
+                              slot=slot_of[entry]))
             ops.append(op)
-        nslots = max(1, len(self._param_entries))
-        ntiles = 1 << (nbits - self.k)
-        partials = torch.empty(2 * nslots * ntiles, dtype=torch.float64, device=self.dev)
-        self._run(psi, nbits, ops, lam=lam, partials=partials)
-        per_inst_tiles = 1 << (self.n - self.k)
-        sums = torch.empty(2 * nslots * bp, dtype=torch.float64, device=self.dev)
-        N.call("qs_segment_sum", C.c_void_p(partials.data_ptr()), nslots * bp, per_inst_tiles,
-               C.c_void_p(sums.data_ptr()), self.stream)
-        self.launches += 1
-        im = sums.view(nslots, bp, 2)[:, :, 1]  # Im <lam|G|psi> per (slot, instance)
-        scale = torch.tensor([self.circuit.entries[e].scale for e in self._param_entries], dtype=torch.float64,
-                             device=self.dev)
-        index = torch.tensor([self.circuit.entries[e].index for e in self._param_entries], dtype=torch.long,
-                             device=self.dev)
-        grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
-        grads.index_add_(0, index, im * scale[:, None])
-        return e[:b], grads.t()[:b]
+        gp.bwd = self._build(nbits, ops, adjoint=True)
+        gp.nslots = max(1, len(self._param_entries))
+        gp.psi = torch.empty(bp << self.n, dtype=self.cdtype, device=self.dev)
+        gp.lam = torch.empty_like(gp.psi)
+        gp.partials = torch.empty(2 * gp.nslots * (1 << (nbits - self.k)), dtype=torch.float64, device=self.dev)
+        gp.sums = torch.empty(2 * gp.nslots * bp, dtype=torch.float64, device=self.dev)
+        gp.e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
+        gp.ws = torch.empty(16 * bp * 64 + 256, dtype=torch.uint8, device=self.dev)
+        # gradient = W @ Im<lam|G|psi>, W[param, slot] = scale: a fixed-order (deterministic)
+        # sum over the gates that share a parameter
+        w = np.zeros((self.circuit.num_params, gp.nslots))
+        for s_, e in enumerate(self._param_entries):
+            w[self.circuit.entries[e].index, s_] += self.circuit.entries[e].scale
+        gp.weights = torch.from_numpy(w).to(self.dev)
+        gp.grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
+        return gp
+
+    def _build(self, nbits: int, ops: Sequence[Op], adjoint: bool):
+        steps = plan(ops, nbits, self.k, self.nlow, merge_bits=0 if adjoint else 2)
+        passes = [s for s in steps if isinstance(s, Pass)]
+        if len(passes) != len(steps):
+            raise RuntimeError("a gradient-circuit op could not be fused")
+        table = MatrixTable()
+        cps, npass, cops, nops = emit(passes, table, inst_shift=self.n)
+        mats = torch.from_numpy(table.array().astype(self.np_dtype)).to(self.dev)
+        return (cps, npass, cops, nops, mats)
+
+    def launch(self, gp: "GradientPlan", stream=None):
+        """Issue the forward, energy and adjoint kernels of a plan on `stream`
+        (default: the current stream).  Results land in gp.e and gp.grads."""
+        st = N.stream_ptr(stream if stream is not None else torch.cuda.current_stream(self.dev))
+        n, bp, nbits = self.n, gp.bp, gp.nbits
+        psi, lam = gp.psi, gp.lam
+        psi.zero_()
+        psi.view(bp, 1 << n)[:, 0] = 1
+        cps, npass, cops, nops, mats = gp.fwd
+        N.call("qs_apply_fused", C.c_void_p(psi.data_ptr()), nbits, qs_dtype(psi), cps, npass, cops, nops,
+               C.c_void_p(mats.data_ptr()), int(mats.numel()), st)
+        x, z, c = self.pauli
+        N.call("qs_apply_pauli_sum", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
+               qs_dtype(psi), x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
+               c.ctypes.data_as(C.c_void_p), len(x), st)
+        N.call("qs_inner_batched", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits, qs_dtype(psi),
+               n, C.c_void_p(gp.e.data_ptr()), C.c_void_p(gp.ws.data_ptr()), gp.ws.numel(), st)
+        cps, npass2, cops, nops, mats = gp.bwd
+        N.call("qs_adjoint_fused", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
+               qs_dtype(psi), cps, npass2, cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
+               C.c_void_p(gp.partials.data_ptr()), int(gp.partials.numel()), st)
+        N.call("qs_segment_sum", C.c_void_p(gp.partials.data_ptr()), gp.nslots * bp, 1 << (n - self.k),
+               C.c_void_p(gp.sums.data_ptr()), st)
+        self.launches += npass + npass2 + 3
+        im = gp.sums.view(gp.nslots, bp, 2)[:, :, 1]
+        torch.matmul(gp.weights, im, out=gp.grads)
+
+    def gradient(self, params) -> Tuple[torch.Tensor, torch.Tensor]:
+        """(energies (B,), gradients (B, P)) in FP64."""
+        gp = self.plan_gradient(params)
+        self.launch(gp)
+        return gp.e.view(gp.bp, 2)[: gp.b, 0], gp.grads.t()[: gp.b]
 
     def parameter_shift(self, params, indices: Optional[Sequence[int]] = None) -> torch.Tensor:
         """Gradient by the two-term shift rule (exact for exp(-i theta G / 2), G^2 = I),
@@ -227,6 +269,21 @@ class BatchedAdjoint:
                 op = Op(op.kind, op.tbits, (), op.mat, tag=op.tag, batch=tab)
             ops.append(op)
         return ops
+
+
+class GradientPlan:
+    """Device buffers and ctypes pass arrays of one planned gradient evaluation."""
+
+    def __init__(self, b: int, bp: int, nbits: int):
+        self.b, self.bp, self.nbits = b, bp, nbits
+
+    @property
+    def energies(self) -> torch.Tensor:
+        return self.e.view(self.bp, 2)[: self.b, 0]
+
+    @property
+    def gradients(self) -> torch.Tensor:
+        return self.grads.t()[: self.b]
 
 
 class _ExpectationFn(torch.autograd.Function):

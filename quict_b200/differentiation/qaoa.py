@@ -1,0 +1,92 @@
+"""Uneven-size batched QAOA MaxCut: energies and adjoint gradients of many
+instances with different qubit counts, graphs and depths, replayed as ONE
+CUDA-graph launch.
+
+Every instance is planned once on the host (``BatchedAdjoint.plan_gradient``:
+gate tables, fused-pass plans, device buffers).  Its kernel chain (forward
+passes, lam = C psi, FP64 energy, adjoint sweep, partial sums) is then
+captured into one graph.  Instances are spread over several capture streams,
+so their chains are independent branches that the GPU runs concurrently:
+small instances (2^10 amplitudes = one tile) fill the SMs side by side, and
+large ones (2^24) use the whole GPU.
+"""
+from __future__ import annotations
+
+from typing import List, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .adjoint import BatchedAdjoint, GradientPlan
+from .circuit import maxcut_observable, qaoa_circuit, random_regular_graph
+
+
+def qaoa_instances(count: int = 512, sizes: Sequence[int] = tuple(range(10, 25, 2)), depths=(1, 6),
+                   seed: int = 4) -> List[Tuple[int, List[Tuple[int, int]], int, np.ndarray]]:
+    """Seeded (n, edges, p, params) tuples: n uniform over `sizes`, p uniform in
+    depths, a random 3-regular graph, gammas and betas uniform in [0, pi)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(sizes[rng.integers(len(sizes))])
+        p = int(rng.integers(depths[0], depths[1] + 1))
+        edges = random_regular_graph(n, 3, rng)
+        params = rng.uniform(0, np.pi, 2 * p)
+        out.append((n, edges, p, params))
+    return out
+
+
+class UnevenQAOABatch:
+    def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16):
+        self.instances = instances
+        self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id)
+                        for n, edges, p, _ in instances]
+        self.plans: List[GradientPlan] = [eng.plan_gradient(np.asarray(prm)[None, :])
+                                          for eng, (_, _, _, prm) in zip(self.engines, instances)]
+        self.dev = self.engines[0].dev if self.engines else torch.device("cuda", device_id)
+        self.nstreams = streams
+        self.graph = None
+
+    @property
+    def num_gradients(self) -> int:
+        return sum(2 * p for _, _, p, _ in self.instances)
+
+    def _launch_all(self, streams):
+        cur = torch.cuda.current_stream(self.dev)
+        for s in streams:
+            s.wait_stream(cur)
+        # largest instances first so they start early
+        order = sorted(range(len(self.plans)), key=lambda i: -self.instances[i][0])
+        for j, i in enumerate(order):
+            st = streams[j % len(streams)]
+            with torch.cuda.stream(st):
+                self.engines[i].launch(self.plans[i], st)
+        for s in streams:
+            cur.wait_stream(s)
+
+    def run_eager(self):
+        streams = [torch.cuda.Stream(self.dev) for _ in range(self.nstreams)]
+        self._launch_all(streams)
+
+    def capture(self):
+        """Warm up once (first-launch configuration happens outside capture),
+        then capture every instance's chain into one CUDA graph."""
+        self.run_eager()
+        torch.cuda.synchronize(self.dev)
+        self.graph = torch.cuda.CUDAGraph()
+        streams = [torch.cuda.Stream(self.dev) for _ in range(self.nstreams)]
+        with torch.cuda.graph(self.graph):
+            self._launch_all(streams)
+        return self.graph
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def results(self) -> List[Tuple[float, np.ndarray]]:
+        """[(energy, gradient (2p,))] per instance (host copies)."""
+        out = []
+        for gp in self.plans:
+            out.append((float(gp.energies[0]), gp.gradients[0].cpu().numpy()))
+        return out

@@ -55,3 +55,13 @@ def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: flo
             g = g(*[float(x) for x in rng.uniform(0, 2 * np.pi, g.params)])
         g | c(pick(g.controls + g.targets))
     return c
+
+
+def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int = 3):
+    """Hardware-efficient ansatz (Ry, Rz on every qubit + CZ ring per layer),
+    H = sum Z_i Z_{i+1} (open chain) + 0.5 sum X_i, params uniform in [0, 2 pi)."""
+    from .differentiation import hardware_efficient_ansatz, ising_observable
+    circ = hardware_efficient_ansatz(n, layers)
+    obs = ising_observable(n)
+    params = np.random.default_rng(seed).uniform(0, 2 * np.pi, (batch, circ.num_params))
+    return circ, obs, params
