@@ -46,13 +46,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """dram bytes per fused-pass launch from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "k_fused_30q_c128.txt")
+def ncu_traffic(n):
+    """dram bytes per fused-pass launch from the committed ncu summary (a
+    26-qubit capture scaled by the amplitudes processed), or None."""
+    p = os.path.join(ROOT, "profiles", "k_fused_reg_config1_c128.txt")
     if not os.path.exists(p):
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) * 2.0 ** (n - 30) if m else None
 
 
 class Clocks:
@@ -209,6 +210,66 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _events_ms(fn, reps):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def grad_bench(ws, rank, local, batch=1024):
+    """Config 3: HEA 16q x 8 layers, 256 params, batch 1024 (split over ranks),
+    H = sum ZZ + 0.5 sum X.  Adjoint gradient (c64, c128) vs the same GPU's
+    parameter shift (2 parameters timed, scaled to 256)."""
+    import torch
+    from quict_b200.differentiation import BatchedAdjoint
+    from quict_b200.workloads import config3_problem
+    circ, obs, params = config3_problem(16, 8, batch)
+    per = batch // ws
+    mine = params[rank * per:(rank + 1) * per]
+    out = {"workload": f"hea-16q-8layers-256params-batch{batch}", "observable": "sum Z_i Z_i+1 (open) + 0.5 sum X_i",
+           "instances_per_rank": per}
+    grads = {}
+    for prec in ("single", "double"):
+        eng = BatchedAdjoint(circ, obs, prec, local)
+        gp = eng.plan_gradient(mine)
+        barrier(ws)
+        ms = max_over_ranks(_events_ms(lambda: eng.launch(gp), 3), ws)
+        grads[prec] = gp.gradients.clone()
+        ps_ms = max_over_ranks(_events_ms(lambda: eng.parameter_shift(mine, indices=[0, 128]), 1), ws) / 2 * 256
+        key = "c64" if prec == "single" else "c128"
+        out[key] = {"ms": ms, "grads_per_s": ws * per * 256 / (ms / 1e3),
+                    "param_shift_ms": ps_ms, "param_shift_note": "2 parameters timed, x128 to 256",
+                    "speedup_vs_param_shift": ps_ms / ms}
+        del gp, eng
+        torch.cuda.empty_cache()
+    out["max_abs_grad_err_c64_vs_c128"] = float((grads["single"] - grads["double"]).abs().max())
+    return out
+
+
+def qaoa_bench(ws, rank, local, count=512):
+    """Config 4: uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6), one CUDA
+    graph per rank (instances split round-robin over ranks), complex64."""
+    import torch
+    from quict_b200.differentiation import UnevenQAOABatch, qaoa_instances
+    inst = qaoa_instances(count)
+    mine = inst[rank::ws]
+    batch = UnevenQAOABatch(mine, "single", local)
+    batch.capture()
+    barrier(ws)
+    ms = max_over_ranks(_events_ms(batch.replay, 3), ws)
+    total_grads = sum(2 * p for _, _, p, _ in inst)
+    return {"workload": f"qaoa-maxcut-{count}instances-n10..24-p1..6", "graph_replay_ms": ms,
+            "grads_per_s": total_grads / (ms / 1e3), "instances_per_s": count / (ms / 1e3),
+            "launches_per_replay": sum(e.launches for e in batch.engines) // 2}
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -302,16 +363,21 @@ def run_ours(args, ws, rank, local):
                    "l2": "inputs larger than L2 (16 GiB state vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "hbm_gbs_effective": npasses * bytes_per_pass / (ms / 1e3) / 1e9,
-        "roofline": {"bound": "hbm", "kernel": "k_fused", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(),
+        "roofline": {"bound": "hbm", "kernel": "k_fused_reg", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(n),
                      "algorithmic_bytes_per_launch": bytes_per_pass, "avg_launch_ms": avg_pass_ms},
         "e2e": {"value": ws * len(ops) / e2e_s, "unit": "gates/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": 8},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if not args.no_grad:
         del sim, vec
+        torch.cuda.empty_cache()
+        line["adjoint"] = grad_bench(ws, rank, local)
+        line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        torch.cuda.empty_cache()
         torch.cuda.empty_cache()
         cb = CpuBaseline(circuit, n)
         r, done, dt = cb.step(0, args.ref_budget, args.ref_gates)
@@ -332,6 +398,8 @@ def main():
     ap.add_argument("--ref-gates", type=int, default=24)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
+    ap.add_argument("--qaoa-instances", type=int, default=512)
     ap.add_argument("--max-pass-cost", type=float, default=float("inf"),
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units")
     args = ap.parse_args()
