@@ -231,8 +231,10 @@ def grad_bench(ws, rank, local, batch=1024):
     from quict_b200.differentiation import BatchedAdjoint
     from quict_b200.workloads import config3_problem
     circ, obs, params = config3_problem(16, 8, batch)
-    per = batch // ws
-    mine = params[rank * per:(rank + 1) * per]
+    from quict_b200.distributed import block_shard
+    rows = block_shard(batch, ws, rank)
+    per = len(rows)
+    mine = params[rows.start:rows.stop]
     out = {"workload": f"hea-16q-8layers-256params-batch{batch}", "observable": "sum Z_i Z_i+1 (open) + 0.5 sum X_i",
            "instances_per_rank": per}
     grads = {}
@@ -255,11 +257,13 @@ def grad_bench(ws, rank, local, batch=1024):
 
 def qaoa_bench(ws, rank, local, count=512):
     """Config 4: uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6), one CUDA
-    graph per rank (instances split round-robin over ranks), complex64."""
+    graph per rank (instances split over ranks by amplitude x depth cost), complex64."""
     import torch
     from quict_b200.differentiation import UnevenQAOABatch, qaoa_instances
+    from quict_b200.distributed import balanced_shard
     inst = qaoa_instances(count)
-    mine = inst[rank::ws]
+    parts = balanced_shard([float(2 ** n) * (p * (1.5 * n + n)) for n, _, p, _ in inst], ws)
+    mine = [inst[i] for i in parts[rank]]
     batch = UnevenQAOABatch(mine, "single", local)
     batch.capture()
     barrier(ws)
