@@ -153,3 +153,17 @@ def permute_qubits(vec: np.ndarray, n: int, dest_from_src: Sequence[int]) -> np.
     """Qubit permutation: new qubit i holds old qubit mapping[i]."""
     t = vec.reshape([2] * n)
     return np.ascontiguousarray(np.transpose(t, list(dest_from_src))).reshape(-1)
+
+
+def vector_permutation(vec: np.ndarray, n: int, mapping) -> np.ndarray:
+    """Index-level restatement of the reference's vector_*_permutation kernel
+    (QuICT/ops/linalg/gpu_calculator.py:170-207): y[t] = x[xid] with bit
+    (n-1-i) of xid taken from bit (n-1-mapping[i]) of t."""
+    x = np.asarray(vec)
+    y = np.empty_like(x)
+    for t in range(1 << n):
+        xid = 0
+        for i in range(n):
+            xid |= ((t >> (n - 1 - mapping[i])) & 1) << (n - 1 - i)
+        y[t] = x[xid]
+    return y

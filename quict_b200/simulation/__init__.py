@@ -1,3 +1,4 @@
 """Simulators: drop-in replacements for QuICT.simulation's GPU backends."""
 from .state_vector import StateVectorSimulator, StateArray  # noqa: F401
 from .density_matrix import DensityMatrixSimulator  # noqa: F401
+from .unitary import UnitarySimulator  # noqa: F401
