@@ -285,7 +285,7 @@ def run_ours(args, ws, rank, local):
     n = args.qubits
     circuit = config1_circuit(n, N_GATES, SEED)
     sim = StateVectorSimulator("GPU", "double", gpu_device_id=local, sync=False,
-                               max_pass_cost=args.max_pass_cost)
+                               max_pass_cost=args.max_pass_cost, merge_bits=args.merge_bits)
     eng = sim.engine
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -403,6 +403,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
+    ap.add_argument("--merge-bits", type=int, default=2, help="gate-merging block width (0 disables)")
     ap.add_argument("--qaoa-instances", type=int, default=512)
     ap.add_argument("--max-pass-cost", type=float, default=float("inf"),
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units")

@@ -317,8 +317,10 @@ struct KOp {
     uint16_t tctrl;   // control mask on the thread's tile bits
     uint16_t moff;    // shared-memory offset of the slot-ordered matrix
     uint8_t flags;
-    uint8_t pad[3];
+    uint8_t ns;       // DIAG: number of slot targets
+    uint8_t pad[2];
     uint64_t gctrl;   // control mask on vector bits outside the tile
+    uint8_t kidx[32]; // DIAG: slot s -> index of its slot bits in the diagonal
 };
 struct KCopy {
     int64_t goff;     // table offset of the stored matrix
@@ -498,6 +500,25 @@ __device__ __forceinline__ void r_diag(V (&x)[E], const V* __restrict__ Dm, uint
     });
 }
 
+// ---- diagonal, one code path for every slot mask: x[s] *= d[(h << ns) | kidx[s]]
+template <typename V, int E>
+__device__ __forceinline__ void r_diag_any(V (&x)[E], const V* __restrict__ Dm, uint32_t scm, uint32_t h,
+                                           const KOp& op) {
+    const V* d = Dm + (h << op.ns);
+    uint32_t kw[E / 4];
+#pragma unroll
+    for (int i = 0; i < E / 4; ++i) kw[i] = reinterpret_cast<const uint32_t*>(op.kidx)[i];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+        const uint32_t k = (kw[s >> 2] >> (8 * (s & 3))) & 0xffu;
+        const V f = d[k];
+        const V y = cmul(x[s], f);
+        const bool ok = (uint32_t(s) & scm) == scm;
+        x[s].x = ok ? y.x : x[s].x;
+        x[s].y = ok ? y.y : x[s].y;
+    }
+}
+
 #define QS_MASKS_1_31(F)                                                                             \
     F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15) F(16) F(17) \
         F(18) F(19) F(20) F(21) F(22) F(23) F(24) F(25) F(26) F(27) F(28) F(29) F(30) F(31)
@@ -526,32 +547,21 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
 #undef QS_CASE
             }
             break;
-        case QS_OP_ANTI:
+        case QS_OP_ANTI:  // the host routes only unit exchanges here
             switch (op.mask) {
 #define QS_CASE(MK)                                                                  \
     case MK:                                                                         \
-        if constexpr ((MK) < (1 << R) && popc_c(MK) == 1) {                          \
-            if (unit) {                                                              \
-                if (pred) r_anti<V, E, MK, true, true>(x, Mm, scm);                  \
-                else r_anti<V, E, MK, false, true>(x, Mm, scm);                      \
-            } else {                                                                 \
-                if (pred) r_anti<V, E, MK, true, false>(x, Mm, scm);                 \
-                else r_anti<V, E, MK, false, false>(x, Mm, scm);                     \
-            }                                                                        \
-        }                                                                            \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) == 1) r_anti<V, E, MK, true, true>(x, Mm, scm); \
         break;
                 QS_MASKS_1_31(QS_CASE)
 #undef QS_CASE
             }
             break;
-        case QS_OP_SWAP:
+        case QS_OP_SWAP:  // the host routes only unit exchanges here
             switch (op.mask) {
 #define QS_CASE(MK)                                                                  \
     case MK:                                                                         \
-        if constexpr ((MK) < (1 << R) && popc_c(MK) == 2) {                          \
-            if (unit) r_swap<V, E, MK, true, true>(x, Mm, scm);                      \
-            else r_swap<V, E, MK, true, false>(x, Mm, scm);                          \
-        }                                                                            \
+        if constexpr ((MK) < (1 << R) && popc_c(MK) == 2) r_swap<V, E, MK, true, true>(x, Mm, scm); \
         break;
                 QS_MASKS_1_31(QS_CASE)
 #undef QS_CASE
@@ -564,23 +574,15 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
                 const uint32_t bit = src < 64 ? (thr >> src) & 1u : uint32_t((base >> (src - 64)) & 1u);
                 h = (h << 1) | bit;
             }
-            switch (op.mask) {
-                case 0:
-                    if (pred) r_diag<V, E, 0, true>(x, Mm, scm, h);
-                    else r_diag<V, E, 0, false>(x, Mm, scm, h);
-                    break;
-#define QS_CASE(MK)                                                                  \
-    case MK:                                                                         \
-        if constexpr ((MK) < (1 << R) && popc_c(MK) <= 4) {                          \
-            if (pred) r_diag<V, E, MK, true>(x, Mm, scm, h);                         \
-            else r_diag<V, E, MK, false>(x, Mm, scm, h);                             \
-        }                                                                            \
-        break;
-                QS_MASKS_1_31(QS_CASE)
-#undef QS_CASE
+            if (op.ns == 0) {  // no target in registers: one factor per thread
+                if (pred) r_diag<V, E, 0, true>(x, Mm, scm, h);
+                else r_diag<V, E, 0, false>(x, Mm, scm, h);
+            } else {
+                r_diag_any<V, E>(x, Mm, scm, h, op);
             }
         }
     }
+    (void)unit;
 }
 
 // thread part (tile bits) of a stage layout
@@ -922,6 +924,9 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegA
         c = KCopy{};
         k.code = uint8_t(op.kind);
         k.flags = uint8_t(op.flags);
+        // only plain exchanges keep their own code paths; scaled anti-diagonal /
+        // swap matrices run as dense matrices (their stored 2x2 / 4x4 is complete)
+        if ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT)) k.code = QS_OP_MAT;
         k.gctrl = op.gctrl;
         uint32_t scm = 0, tct = 0;
         for (int b = 0; b < K; ++b)
@@ -969,6 +974,13 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegA
         }
         k.mask = uint8_t(mask);
         k.nh = uint8_t(nh);
+        k.ns = uint8_t(ns_);
+        for (int sidx = 0; sidx < (1 << R) && sidx < 32; ++sidx) {
+            int kv = 0;
+            for (int x2 = 0; x2 < ns_; ++x2)
+                if ((sidx >> slots[x2]) & 1) kv |= 1 << x2;
+            k.kidx[sidx] = uint8_t(kv);
+        }
         moff += msize;
         ++nops;
         ++S.op_count;
