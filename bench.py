@@ -223,6 +223,48 @@ def _events_ms(fn, reps):
     return a.elapsed_time(b) / reps
 
 
+def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=2):
+    """Device-timed gates/s of the config-1 circuit at n qubits (extra precisions / sizes)."""
+    import torch
+    from quict_b200 import _native as N
+    from quict_b200.simulation import StateVectorSimulator
+    from quict_b200.simulation.fusion import Pass
+    from quict_b200.simulation.lowering import lower_circuit
+    from quict_b200.workloads import config1_circuit
+    circuit = config1_circuit(n, N_GATES, SEED)
+    sim = StateVectorSimulator("GPU", precision, gpu_device_id=local, sync=False, merge_bits=merge_bits)
+    eng = sim.engine
+    ops = lower_circuit(circuit.gates, n)
+    sim.initial_circuit(circuit)
+    sim.initial_state_vector()
+    vec = sim._vector
+    plan_ = eng.plan(vec, n, ops)
+    dt = N.QS_C128 if precision == "double" else N.QS_C64
+
+    def step():
+        N.call("qs_init_zero", vec.data_ptr(), n, dt, eng.stream)
+        batch = []
+        for st in plan_:
+            if isinstance(st, Pass):
+                batch.append(st)
+            else:
+                eng.run_passes(vec, n, batch)
+                batch = []
+                eng.apply_single(vec, n, st.op)
+        eng.run_passes(vec, n, batch)
+
+    for _ in range(warmup):
+        step()
+    barrier(ws)
+    ms = max_over_ranks(_events_ms(step, steps), ws)
+    passes = sum(1 for s in plan_ if isinstance(s, Pass) and s.ops)
+    del sim, vec
+    torch.cuda.empty_cache()
+    return {"workload": f"sv-{n}q-{'c128' if precision == 'double' else 'c64'}-{N_GATES}g-config1",
+            "gates_per_s": ws * len(ops) / (ms / 1e3), "ms_per_run": ms, "fused_passes": passes,
+            "state_bytes": (1 << n) * (16 if precision == "double" else 8)}
+
+
 def grad_bench(ws, rank, local, batch=1024):
     """Config 3: HEA 16q x 8 layers, 256 params, batch 1024 (split over ranks),
     H = sum ZZ + 0.5 sum X.  Adjoint gradient (c64, c128) vs the same GPU's
@@ -375,13 +417,14 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    del sim, vec
+    torch.cuda.empty_cache()
+    if not args.no_extra:
+        line["c64"] = [sv_rate(30, "single", local, ws), sv_rate(32, "single", local, ws)]
     if not args.no_grad:
-        del sim, vec
-        torch.cuda.empty_cache()
         line["adjoint"] = grad_bench(ws, rank, local)
         line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        torch.cuda.empty_cache()
         torch.cuda.empty_cache()
         cb = CpuBaseline(circuit, n)
         r, done, dt = cb.step(0, args.ref_budget, args.ref_gates)
@@ -404,6 +447,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
     ap.add_argument("--merge-bits", type=int, default=2, help="gate-merging block width (0 disables)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the complex64 30q / 32q runs")
     ap.add_argument("--qaoa-instances", type=int, default=512)
     ap.add_argument("--max-pass-cost", type=float, default=float("inf"),
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units")
