@@ -316,6 +316,64 @@ def qaoa_bench(ws, rank, local, count=512):
             "launches_per_replay": sum(e.launches for e in batch.engines) // 2}
 
 
+SWEEP_1Q = ("h", "x", "rx", "ry", "rz", "u3")
+SWEEP_2Q = ("cx", "cz", "rzz", "swap")
+
+
+SECTOR = 32  # bytes: the L2 / DRAM sector, the smallest unit a skipped run can save
+
+
+def sweep_bytes(name, bits, n, esize):
+    """Bytes a per-gate kernel must move: every 32-byte sector holding an
+    amplitude it changes is read and written once.  CX changes the control=1
+    half, Swap the |01>,|10> half and CZ the |11> quarter (entries equal to 1
+    are skipped); a skipped half saves traffic only when its runs (2^bit
+    amplitudes) span whole sectors.  The other gates change every amplitude."""
+    def halves(b):
+        return 0.5 if (1 << b) * esize >= SECTOR else 1.0
+    if name == "cx":
+        frac = halves(bits[0])
+    elif name == "cz":
+        frac = halves(bits[0]) * halves(bits[1])
+    elif name == "swap":
+        frac = halves(min(bits))
+    else:
+        frac = 1.0
+    return int(2 * (1 << n) * esize * frac)
+
+
+def gate_sweep(eng, vec, n, ws, reps=5, warmup=2):
+    """Single-gate sweep: each gate class of the config-1 gate set applied by
+    its per-gate kernel to the resident n-qubit state at a low (in-warp), a
+    middle and the highest vector bit; device-timed per launch; GB/s from
+    ``sweep_bytes`` against the measured HBM copy bandwidth."""
+    import torch
+    from quict_b200.core import GATE_BY_NAME
+    from quict_b200.simulation.lowering import lower_gate
+    peak, kind = peaks()
+    esize = vec.element_size()
+    rows = []
+    for name in SWEEP_1Q + SWEEP_2Q:
+        g = GATE_BY_NAME[name]
+        if g.params:
+            g = g(*[0.3 + 0.1 * i for i in range(g.params)])
+        two = name in SWEEP_2Q
+        # (vector bits) -> circuit qubits (qubit q is vector bit n-1-q)
+        for bits in ([(1, 0), (14, 3), (n - 1, n - 2)] if two else [(0,), (14,), (n - 1,)]):
+            (op,) = lower_gate(g & [n - 1 - b for b in bits], n)
+            for _ in range(warmup):
+                eng.apply_single(vec, n, op)
+            ms = max_over_ranks(_events_ms(lambda: eng.apply_single(vec, n, op), reps), ws)
+            gbs = sweep_bytes(name, bits, n, esize) / (ms / 1e3) / 1e9
+            rows.append({"gate": name, "vector_bits": list(bits), "ms": round(ms, 4),
+                         "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)})
+    fr = sorted(r["frac"] for r in rows)
+    return {"workload": f"sv-{n}q-{'c128' if esize == 16 else 'c64'} one gate per launch",
+            "peak_gbs": peak, "peak_source": kind, "min_frac": fr[0], "median_frac": fr[len(fr) // 2],
+            "bytes_rule": "read+write of the 32-byte sectors holding amplitudes the gate changes",
+            "rows": rows}
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -417,6 +475,8 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if not args.no_extra:
+        line["single_gate_sweep"] = gate_sweep(eng, vec, n, ws)
     del sim, vec
     torch.cuda.empty_cache()
     if not args.no_extra:

@@ -13,7 +13,8 @@
 //   (lanes first).  Ops whose dense targets are slot bits run as fully
 //   unrolled register code (one template per slot mask, no shared memory, no
 //   barriers); between groups of ops ("stages") the tile is re-laid-out
-//   through XOR-swizzled shared memory.  Loads and stores use a layout whose
+//   through shared memory under a per-relayout XOR address map that keeps
+//   both sides free of bank conflicts.  Loads and stores use a layout whose
 //   lanes are tile bits 0..4, i.e. warp-contiguous global runs.  The host
 //   (this file) plans the stages, translates each op into slot / thread /
 //   outside-tile terms and permutes its matrix to the slot order.
@@ -330,10 +331,17 @@ struct KCopy {
     uint8_t diag;
     uint8_t perm[4];  // slot-order index bit i -> stored index bit perm[i]
 };
-struct KStage {
+struct __align__(16) KStage {
+    // Buffer addresses for the relayout into this stage, under a linear (XOR)
+    // map chosen on the host so that the writing and the reading layout both
+    // spread each shared-memory phase over all banks: images of the previous
+    // stage's thread bits / slot bits (writes) and of this stage's (reads).
+    uint16_t wthr[8], rthr[8], wslot[8], rslot[8];
+    uint16_t tbit[8]; // 1 << T[i]: this stage's thread bits as tile positions
     uint8_t R[6];     // slot bit j <-> tile bit R[j]
     uint8_t T[8];     // thread bit i <-> tile bit T[i]
     uint16_t op_begin, op_count;
+    uint16_t img[QS_MAX_TILE_BITS];  // the map itself: buffer address of each tile bit
 };
 struct RegArgs {
     int n, K, L, H, nT, nstages, nops, nmats, inst_shift, batched;
@@ -342,12 +350,6 @@ struct RegArgs {
     KOp ops[QS_MAX_PASS_OPS];
     KCopy cp[QS_MAX_PASS_OPS];
 };
-
-template <typename V>
-__device__ __forceinline__ uint32_t swz(uint32_t t) {
-    if (sizeof(V) == 16) return t ^ (((t >> 3) ^ (t >> 6) ^ (t >> 9) ^ (t >> 12)) & 7u);
-    return t ^ (((t >> 4) ^ (t >> 8) ^ (t >> 12)) & 15u);
-}
 
 __device__ __forceinline__ bool ctrl_ok(int s, uint32_t scm) { return (uint32_t(s) & scm) == scm; }
 
@@ -585,33 +587,38 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
     (void)unit;
 }
 
-// thread part (tile bits) of a stage layout
-template <int R>
-__device__ __forceinline__ uint32_t thread_bits(const KStage& S, int nT) {
+// tile position of this thread's slot 0: XOR of the given images of the set
+// thread-index bits (unrolled; images of unused bits are 0)
+__device__ __forceinline__ uint32_t thread_pos(const uint16_t* __restrict__ img) {
+    const uint4 w = *reinterpret_cast<const uint4*>(img);
+    const uint32_t v[4] = {w.x, w.y, w.z, w.w};
     uint32_t t = 0;
-    for (int i = 0; i < nT; ++i)
-        if ((threadIdx.x >> i) & 1) t |= 1u << S.T[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t im = (v[i >> 1] >> (16 * (i & 1))) & 0xffffu;
+        t ^= ((threadIdx.x >> i) & 1u) ? im : 0u;
+    }
     return t;
 }
 
-template <typename V, int R>
-__device__ __forceinline__ Addr<R> stage_addr(const KStage& S, int nT, bool swizzled) {
+template <int R>
+__device__ __forceinline__ Addr<R> make_addr(const uint16_t* __restrict__ thr_img, const uint16_t* __restrict__ slot_img) {
     Addr<R> a;
-    const uint32_t t = thread_bits<R>(S, nT);
-    a.tpos = swizzled ? swz<V>(t) : t;
+    a.tpos = thread_pos(thr_img);
+    const uint4 w = *reinterpret_cast<const uint4*>(slot_img);
+    const uint32_t v[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-    for (int j = 0; j < R; ++j) a.rpos[j] = swizzled ? swz<V>(1u << S.R[j]) : (1u << S.R[j]);
+    for (int j = 0; j < R; ++j) a.rpos[j] = (v[j >> 1] >> (16 * (j & 1))) & 0xffffu;
     return a;
 }
 
-// Re-layout the registers from the current addressing `from` into stage B's
-// (swizzled) addressing; returns B's addressing.
+// Re-layout the registers from the previous stage's layout into stage B's
+// through the buffer under B's map; returns B's addressing.
 template <typename V, int R>
-__device__ __forceinline__ Addr<R> r_relayout(V (&x)[1 << R], V* __restrict__ buf, const KStage& A, const KStage& B,
-                                              int nT) {
+__device__ __forceinline__ Addr<R> r_relayout(V (&x)[1 << R], V* __restrict__ buf, const KStage& B) {
     constexpr int E = 1 << R;
-    const Addr<R> aw = stage_addr<V, R>(A, nT, true);
-    const Addr<R> ar = stage_addr<V, R>(B, nT, true);
+    const Addr<R> aw = make_addr<R>(B.wthr, B.wslot);
+    const Addr<R> ar = make_addr<R>(B.rthr, B.rslot);
     __syncthreads();  // previous readers of buf are done
     sfor<E>([&](auto sc) __attribute__((always_inline)) {
         constexpr int s = decltype(sc)::value;
@@ -660,7 +667,7 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     // op and stage descriptors live in shared memory: the per-op loop reads
     // them with a data-dependent index, which the constant cache serves poorly
     KOp* sops = reinterpret_cast<KOp*>(gslot_store + E);
-    KStage* sst = reinterpret_cast<KStage*>(sops + p.nops);
+    KStage* sst = reinterpret_cast<KStage*>((reinterpret_cast<uintptr_t>(sops + p.nops) + 15) & ~uintptr_t(15));
     for (int o = threadIdx.x; o < p.nops; o += blockDim.x) sops[o] = p.ops[o];
     for (int o = threadIdx.x; o < p.nstages; o += blockDim.x) sst[o] = p.st[o];
     // stage the pass's matrices in slot order (per instance when batched)
@@ -725,15 +732,15 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
         }
         V x[E];
         // shared memory -> registers in the first stage's (plain) layout
-        Addr<R> ad = stage_addr<V, R>(sst[0], nT, false);
+        Addr<R> ad = make_addr<R>(sst[0].rthr, sst[0].rslot);  // stage 0: identity map
         sfor<E>([&](auto sc) __attribute__((always_inline)) {
             constexpr int s = decltype(sc)::value;
             x[s] = cur[ad.template at<s>()];
         });
         for (int si = 0; si < p.nstages; ++si) {
             const KStage& S = sst[si];
-            if (si > 0) ad = r_relayout<V, R>(x, cur, sst[si - 1], S, nT);
-            const uint32_t thr = thread_bits<R>(S, nT);
+            if (si > 0) ad = r_relayout<V, R>(x, cur, S);
+            const uint32_t thr = thread_pos(S.tbit);
             const int oe = S.op_begin + S.op_count;
             for (int o = S.op_begin; o < oe; ++o) {
                 const KOp& op = sops[o];
@@ -843,10 +850,70 @@ int launch_smem(V* vec, V* vec2, int n, const qs_pass& ps, const qs_op* ops, con
     return QS_OK;
 }
 
+// Buffer map of a relayout from layout A to layout B.  Shared memory serves
+// a warp's access in phases of 2^nb lanes (thread bits 0..nb-1; 8 lanes for
+// 16-byte elements, 16 for 8-byte ones); a phase is conflict-free when its
+// lanes' elements fall in distinct 2^nb-element bank groups, i.e. when the map
+// sends the phase's tile bits to independent vectors of the low nb address
+// bits.  The map keeps every address bit and XORs a host-chosen column H[b]
+// into the bank bits for each tile bit b >= nb (invertible: unitriangular);
+// H is searched so that both A's and B's phase bits are independent.
+void relayout_map(const KStage& A, KStage& B, int K, int nb) {
+    int H[QS_MAX_TILE_BITS] = {0};
+    int vars[16], nv = 0;
+    auto add_var = [&](int b) {
+        if (b < nb) return;
+        for (int i = 0; i < nv; ++i)
+            if (vars[i] == b) return;
+        vars[nv++] = b;
+    };
+    for (int i = 0; i < nb; ++i) add_var(A.T[i]);
+    for (int i = 0; i < nb; ++i) add_var(B.T[i]);
+    auto col = [&](int b) { return b < nb ? (1 << b) : H[b]; };
+    // are the already-known phase columns of layout S linearly independent?
+    auto indep = [&](const KStage& S, int assigned) {
+        int basis[8] = {0};  // basis[k]: stored vector whose leading bit is k
+        for (int i = 0; i < nb; ++i) {
+            const int b = S.T[i];
+            bool known = b < nb;
+            for (int v = 0; v < assigned && !known; ++v) known = vars[v] == b;
+            if (!known) continue;
+            int c = col(b);
+            for (int k = nb - 1; k >= 0 && c; --k) {
+                if (!((c >> k) & 1)) continue;
+                if (!basis[k]) {
+                    basis[k] = c;
+                    break;
+                }
+                c ^= basis[k];
+            }
+            if (c == 0) return false;
+        }
+        return true;
+    };
+    long budget = 200000;
+    bool ok = false;
+    // depth-first search over the columns of the phase bits
+    auto dfs = [&](auto&& self, int v) -> bool {
+        if (--budget < 0) return false;
+        if (v == nv) return true;
+        for (int c = 1; c < (1 << nb); ++c) {
+            H[vars[v]] = c;
+            if (indep(A, v + 1) && indep(B, v + 1) && self(self, v + 1)) return true;
+        }
+        H[vars[v]] = 0;
+        return false;
+    };
+    ok = dfs(dfs, 0);
+    if (!ok)
+        for (int b = 0; b < QS_MAX_TILE_BITS; ++b) H[b] = 0;
+    for (int b = 0; b < QS_MAX_TILE_BITS; ++b) B.img[b] = uint16_t(b < K ? ((1 << b) ^ (b >= nb ? H[b] : 0)) : 0);
+}
+
 // Build the register-kernel arguments for ops [first, ...) of a pass; returns
 // the number of ops consumed (a pass whose stages or matrices overflow the
 // argument block is split into several launches over the same tile).
-int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegArgs& a) {
+int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, int nb, RegArgs& a) {
     const int K = ps.k, L = ps.nlow, nT = K - R;
     a.n = n; a.K = K; a.L = L; a.H = K - L; a.nT = nT;
     a.inst_shift = ps.inst_shift;
@@ -996,6 +1063,19 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, RegA
         a.st[ns].op_count = 0;
         ++ns;
     }
+    for (int b = 0; b < QS_MAX_TILE_BITS; ++b) a.st[0].img[b] = uint16_t(b < K ? 1 << b : 0);
+    for (int si = 1; si < ns; ++si) relayout_map(a.st[si - 1], a.st[si], K, nb);
+    for (int si = 0; si < ns; ++si) {
+        KStage& S = a.st[si];
+        const KStage& P = a.st[si > 0 ? si - 1 : 0];
+        for (int i = 0; i < 8; ++i) {
+            S.wthr[i] = i < nT ? S.img[P.T[i]] : 0;
+            S.rthr[i] = i < nT ? S.img[S.T[i]] : 0;
+            S.tbit[i] = i < nT ? uint16_t(1u << S.T[i]) : 0;
+            S.wslot[i] = i < R ? S.img[P.R[i]] : 0;
+            S.rslot[i] = i < R ? S.img[S.R[i]] : 0;
+        }
+    }
     a.nstages = ns;
     a.nops = nops;
     a.nmats = moff;
@@ -1008,13 +1088,14 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
     config_smem((const void*)k_fused_reg<V, R>);
     int first = 0;
     while (first < ps.op_count) {
-        int used = build_reg(ps, ops, first, n, R, args);
+        // bank-group bits of a shared-memory phase: 8 x 16-byte or 16 x 8-byte elements
+        int used = build_reg(ps, ops, first, n, R, sizeof(V) == 16 ? 3 : 4, args);
         if (used <= 0) {
             set_error("qs_apply_fused: op %d does not fit a register tile", ps.op_begin + first);
             return QS_EINVAL;
         }
         size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
-                      sizeof(KOp) * args.nops + sizeof(KStage) * args.nstages;
+                      sizeof(KOp) * args.nops + 16 + sizeof(KStage) * args.nstages;
         uint64_t ntiles = uint64_t(1) << (n - ps.k);
         uint64_t cap = uint64_t(sm_count());
         k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), 1 << (ps.k - R), smem, st>>>(vec, args, mats);
@@ -1032,7 +1113,7 @@ int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
     constexpr int R = reg_bits<V>();
     const int nT = ps.k - R;
     const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
-                        sizeof(KOp) * QS_MAX_PASS_OPS + sizeof(KStage) * kMaxStages;
+                        sizeof(KOp) * QS_MAX_PASS_OPS + 16 + sizeof(KStage) * kMaxStages;
     if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
     return launch_smem<V, false>(vec, nullptr, n, ps, ops, mats, nullptr, st);
 }
