@@ -23,6 +23,7 @@
 // The reference has no fusion: one kernel and one full HBM pass per gate
 // (statevector_simulator.py:155-164, gate_function.py:31-1031).
 #include <algorithm>
+#include <array>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -910,155 +911,201 @@ void relayout_map(const KStage& A, KStage& B, int K, int nb) {
     for (int b = 0; b < QS_MAX_TILE_BITS; ++b) B.img[b] = uint16_t(b < K ? ((1 << b) ^ (b >= nb ? H[b] : 0)) : 0);
 }
 
-// Build the register-kernel arguments for ops [first, ...) of a pass; returns
-// the number of ops consumed (a pass whose stages or matrices overflow the
-// argument block is split into several launches over the same tile).
-int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, int nb, RegArgs& a) {
+// Build the register-kernel arguments for the ops of a pass listed in `rem`
+// (positions within the pass); returns how many were scheduled and removes
+// them from `rem` (a pass whose stages or matrices overflow the argument block
+// is split into several launches over the same tiles).
+//
+// Stage schedule: the ops form a dependency graph (two ops stay ordered when
+// one acts non-diagonally on a tile bit the other touches; all other pairs
+// commute).  A stage holds R tile bits in registers and runs every op whose
+// dense targets it holds once the op's predecessors have run.  Stages are
+// chosen greedily: every R-bit set is scored by the number of ops it would
+// run; ties prefer sets off the lane bits (no extra store relayout).
+int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n, int R, int nb, RegArgs& a) {
     const int K = ps.k, L = ps.nlow, nT = K - R;
     a.n = n; a.K = K; a.L = L; a.H = K - L; a.nT = nT;
     a.inst_shift = ps.inst_shift;
     a.batched = 0;
     for (int t = 0; t < QS_MAX_TILE_BITS; ++t) a.hi[t] = t < K - L ? ps.hi[t] : 0;
     const int lowlanes = 5;  // tile bits 0..4 are the lanes of the load/store layout
-    auto xbits = [&](const qs_op& op) {
-        std::vector<int> v;
-        if (op.kind != QS_OP_DIAG)
-            for (int j = 0; j < op.m; ++j) v.push_back(op.tgt[j]);
-        return v;
-    };
-    auto make_stage = [&](const std::vector<int>& regs, KStage& S) {
-        for (int j = 0; j < 6; ++j) S.R[j] = j < R ? uint8_t(regs[j]) : 0;
-        int i = 0;
-        for (int b = 0; b < K; ++b)
-            if (std::find(regs.begin(), regs.end(), b) == regs.end()) S.T[i++] = uint8_t(b);
+    const uint32_t lanemask = (1u << lowlanes) - 1u;
+    auto make_stage = [&](uint32_t bits, KStage& S) {
+        int j = 0, i = 0;
+        for (int b = 0; b < K; ++b) {
+            if ((bits >> b) & 1) S.R[j++] = uint8_t(b);
+            else S.T[i++] = uint8_t(b);
+        }
+        for (; j < 6; ++j) S.R[j] = 0;
         for (; i < 8; ++i) S.T[i] = 0;
     };
-    const int count = ps.op_count - first;
-    // initial (load) layout: register bits among tile bits >= 5, preferring early targets
-    std::vector<int> cur;
-    for (int i = 0; i < count && int(cur.size()) < R; ++i)
-        for (int b : xbits(ops[ps.op_begin + first + i]))
-            if (b >= lowlanes && int(cur.size()) < R && std::find(cur.begin(), cur.end(), b) == cur.end())
-                cur.push_back(b);
-    for (int b = K - 1; b >= lowlanes && int(cur.size()) < R; --b)
-        if (std::find(cur.begin(), cur.end(), b) == cur.end()) cur.push_back(b);
-    const std::vector<int> load_layout = cur;
-    int ns = 0, nops = 0, moff = 0;
-    make_stage(cur, a.st[0]);
-    a.st[0].op_begin = 0;
-    a.st[0].op_count = 0;
-    ns = 1;
-    int consumed = 0;
-    for (int i = 0; i < count; ++i) {
-        const qs_op& op = ops[ps.op_begin + first + i];
-        const int msize = op.kind == QS_OP_DIAG ? (1 << op.m) : (1 << (2 * op.m));
-        if (moff + msize > QS_MAX_PASS_MATS) break;
-        std::vector<int> xb = xbits(op);
-        bool fits = true;
-        for (int b : xb)
-            if (std::find(cur.begin(), cur.end(), b) == cur.end()) fits = false;
-        if (!fits) {
-            if (ns + 2 > kMaxStages) break;  // keep room for a final store layout
-            std::vector<int> nx = xb;
-            for (int k2 = i + 1; k2 < count; ++k2) {
-                std::vector<int> xb2 = xbits(ops[ps.op_begin + first + k2]);
-                std::vector<int> u = nx;
-                for (int b : xb2)
-                    if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
-                if (int(u.size()) > R) break;
-                nx = u;
+    // ---- dependency graph
+    const int m = int(rem.size());
+    using Set = std::array<uint64_t, (QS_MAX_PASS_OPS + 63) / 64>;
+    std::vector<uint32_t> xm(m), am(m);
+    std::vector<int> msz(m);
+    std::vector<Set> pred(m);
+    for (int i = 0; i < m; ++i) {
+        const qs_op& op = ops[ps.op_begin + rem[i]];
+        uint32_t x = 0, all = op.lctrl;
+        for (int j = 0; j < op.m; ++j)
+            if (op.tgt[j] >= 0) {
+                all |= 1u << op.tgt[j];
+                if (op.kind != QS_OP_DIAG) x |= 1u << op.tgt[j];
             }
-            for (int b : cur)
-                if (int(nx.size()) < R && std::find(nx.begin(), nx.end(), b) == nx.end()) nx.push_back(b);
-            for (int b = K - 1; b >= 0 && int(nx.size()) < R; --b)
-                if (std::find(nx.begin(), nx.end(), b) == nx.end()) nx.push_back(b);
-            cur = nx;
-            make_stage(cur, a.st[ns]);
-            a.st[ns].op_begin = uint16_t(nops);
-            a.st[ns].op_count = 0;
-            ++ns;
-        }
-        // translate the op into the current layout
-        KStage& S = a.st[ns - 1];
-        auto slot_of = [&](int b) {
-            for (int j = 0; j < R; ++j)
-                if (S.R[j] == b) return j;
-            return -1;
-        };
-        KOp& k = a.ops[nops];
-        KCopy& c = a.cp[nops];
-        k = KOp{};
-        c = KCopy{};
-        k.code = uint8_t(op.kind);
-        k.flags = uint8_t(op.flags);
-        // only plain exchanges keep their own code paths; scaled anti-diagonal /
-        // swap matrices run as dense matrices (their stored 2x2 / 4x4 is complete)
-        if ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT)) k.code = QS_OP_MAT;
-        k.gctrl = op.gctrl;
-        uint32_t scm = 0, tct = 0;
-        for (int b = 0; b < K; ++b)
-            if ((op.lctrl >> b) & 1) {
-                int sl = slot_of(b);
-                if (sl >= 0) scm |= 1u << sl;
-                else tct |= 1u << b;
+        xm[i] = x;
+        am[i] = all;
+        msz[i] = op.kind == QS_OP_DIAG ? (1 << op.m) : (1 << (2 * op.m));
+        pred[i].fill(0);
+        for (int h = 0; h < i; ++h)
+            if ((xm[h] & am[i]) | (am[h] & xm[i])) pred[i][h >> 6] |= uint64_t(1) << (h & 63);
+    }
+    auto has = [](const Set& d, int i) { return (d[i >> 6] >> (i & 63)) & 1; };
+    auto ready = [&](const Set& d, int i) {
+        for (size_t w = 0; w < d.size(); ++w)
+            if (pred[i][w] & ~d[w]) return false;
+        return true;
+    };
+    // ops a stage holding `bits` runs from state d (one forward sweep: every
+    // predecessor has a smaller position)
+    auto score = [&](uint32_t bits, Set d) {
+        int c = 0;
+        for (int i = 0; i < m; ++i)
+            if (!has(d, i) && !(xm[i] & ~bits) && ready(d, i)) {
+                d[i >> 6] |= uint64_t(1) << (i & 63);
+                ++c;
             }
-        k.scm = uint8_t(scm);
-        k.tctrl = uint16_t(tct);
-        c.goff = op.mat;
-        c.stride = op.mat_stride;
-        if (op.mat_stride != 0) a.batched = 1;
-        c.soff = uint16_t(moff);
-        c.m = uint8_t(op.m);
-        c.diag = op.kind == QS_OP_DIAG;
-        k.moff = uint16_t(moff);
-        // slot-ordered bit permutation
-        int slots[4], js[4], ns_ = 0;
-        int hj[4], nh = 0;
-        for (int j = 0; j < op.m; ++j) {
-            int sl = op.tgt[j] >= 0 ? slot_of(op.tgt[j]) : -1;
-            if (sl >= 0) {
-                slots[ns_] = sl;
-                js[ns_++] = j;
-            } else {
-                hj[nh++] = j;
-            }
-        }
-        for (int x = 0; x < ns_; ++x)  // sort by slot position
-            for (int y = 0; y + 1 < ns_ - x; ++y)
-                if (slots[y] > slots[y + 1]) {
-                    std::swap(slots[y], slots[y + 1]);
-                    std::swap(js[y], js[y + 1]);
+        return c;
+    };
+    Set done;
+    done.fill(0);
+    int ndone = 0, mats = 0;
+    bool full = false;
+    std::vector<uint32_t> stage_bits;
+    std::vector<std::vector<int>> stage_ops;
+    while (ndone < m && !full && int(stage_bits.size()) < kMaxStages - 1) {
+        const bool first_stage = stage_bits.empty();
+        uint32_t best = 0;
+        int best_score = -1;
+        for (uint32_t bits = (1u << R) - 1u; bits < (1u << K);) {
+            if (!(first_stage && (bits & lanemask))) {
+                const int sc = 2 * score(bits, done) + ((bits & lanemask) == 0);
+                if (sc > best_score && (sc >= 2 || first_stage)) {
+                    best_score = sc;
+                    best = bits;
                 }
-        uint32_t mask = 0;
-        for (int x = 0; x < ns_; ++x) {
-            mask |= 1u << slots[x];
-            c.perm[x] = uint8_t(op.m - 1 - js[x]);
+            }
+            const uint32_t c = bits & (0u - bits), r = bits + c;  // next set of R bits
+            bits = (((r ^ bits) >> 2) / c) | r;
         }
-        for (int q = 0; q < nh; ++q) {
-            c.perm[ns_ + (nh - 1 - q)] = uint8_t(op.m - 1 - hj[q]);
-            const int j = hj[q];
-            k.hsrc[q] = op.tgt[j] >= 0 ? uint8_t(op.tgt[j]) : uint8_t(64 + op.gbit[j]);
+        if (best_score < 0) break;
+        std::vector<int> order;
+        for (int i = 0; i < m; ++i)
+            if (!has(done, i) && !(xm[i] & ~best) && ready(done, i)) {
+                if (mats + msz[i] > QS_MAX_PASS_MATS) {
+                    full = true;
+                    continue;
+                }
+                mats += msz[i];
+                done[i >> 6] |= uint64_t(1) << (i & 63);
+                order.push_back(i);
+                ++ndone;
+            }
+        if (order.empty() && !first_stage) break;
+        stage_bits.push_back(best);
+        stage_ops.push_back(order);
+    }
+    // ---- emit stages and translate each op into its stage's layout
+    int ns = 0, nops = 0, moff = 0;
+    for (size_t st = 0; st < stage_bits.size(); ++st) {
+        make_stage(stage_bits[st], a.st[ns]);
+        a.st[ns].op_begin = uint16_t(nops);
+        a.st[ns].op_count = 0;
+        ++ns;
+        for (int pos : stage_ops[st]) {
+            const qs_op& op = ops[ps.op_begin + rem[pos]];
+            const int msize = msz[pos];
+            // translate the op into the current layout
+            KStage& S = a.st[ns - 1];
+            auto slot_of = [&](int b) {
+                for (int j = 0; j < R; ++j)
+                    if (S.R[j] == b) return j;
+                return -1;
+            };
+            KOp& k = a.ops[nops];
+            KCopy& c = a.cp[nops];
+            k = KOp{};
+            c = KCopy{};
+            k.code = uint8_t(op.kind);
+            k.flags = uint8_t(op.flags);
+            // only plain exchanges keep their own code paths; scaled anti-diagonal /
+            // swap matrices run as dense matrices (their stored 2x2 / 4x4 is complete)
+            if ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT)) k.code = QS_OP_MAT;
+            k.gctrl = op.gctrl;
+            uint32_t scm = 0, tct = 0;
+            for (int b = 0; b < K; ++b)
+                if ((op.lctrl >> b) & 1) {
+                    int sl = slot_of(b);
+                    if (sl >= 0) scm |= 1u << sl;
+                    else tct |= 1u << b;
+                }
+            k.scm = uint8_t(scm);
+            k.tctrl = uint16_t(tct);
+            c.goff = op.mat;
+            c.stride = op.mat_stride;
+            if (op.mat_stride != 0) a.batched = 1;
+            c.soff = uint16_t(moff);
+            c.m = uint8_t(op.m);
+            c.diag = op.kind == QS_OP_DIAG;
+            k.moff = uint16_t(moff);
+            // slot-ordered bit permutation
+            int slots[4], js[4], ns_ = 0;
+            int hj[4], nh = 0;
+            for (int j = 0; j < op.m; ++j) {
+                int sl = op.tgt[j] >= 0 ? slot_of(op.tgt[j]) : -1;
+                if (sl >= 0) {
+                    slots[ns_] = sl;
+                    js[ns_++] = j;
+                } else {
+                    hj[nh++] = j;
+                }
+            }
+            for (int x = 0; x < ns_; ++x)  // sort by slot position
+                for (int y = 0; y + 1 < ns_ - x; ++y)
+                    if (slots[y] > slots[y + 1]) {
+                        std::swap(slots[y], slots[y + 1]);
+                        std::swap(js[y], js[y + 1]);
+                    }
+            uint32_t mask = 0;
+            for (int x = 0; x < ns_; ++x) {
+                mask |= 1u << slots[x];
+                c.perm[x] = uint8_t(op.m - 1 - js[x]);
+            }
+            for (int q = 0; q < nh; ++q) {
+                c.perm[ns_ + (nh - 1 - q)] = uint8_t(op.m - 1 - hj[q]);
+                const int j = hj[q];
+                k.hsrc[q] = op.tgt[j] >= 0 ? uint8_t(op.tgt[j]) : uint8_t(64 + op.gbit[j]);
+            }
+            k.mask = uint8_t(mask);
+            k.nh = uint8_t(nh);
+            k.ns = uint8_t(ns_);
+            for (int sidx = 0; sidx < (1 << R) && sidx < 32; ++sidx) {
+                int kv = 0;
+                for (int x2 = 0; x2 < ns_; ++x2)
+                    if ((sidx >> slots[x2]) & 1) kv |= 1 << x2;
+                k.kidx[sidx] = uint8_t(kv);
+            }
+            moff += msize;
+            ++nops;
+            ++S.op_count;
         }
-        k.mask = uint8_t(mask);
-        k.nh = uint8_t(nh);
-        k.ns = uint8_t(ns_);
-        for (int sidx = 0; sidx < (1 << R) && sidx < 32; ++sidx) {
-            int kv = 0;
-            for (int x2 = 0; x2 < ns_; ++x2)
-                if ((sidx >> slots[x2]) & 1) kv |= 1 << x2;
-            k.kidx[sidx] = uint8_t(kv);
-        }
-        moff += msize;
-        ++nops;
-        ++S.op_count;
-        ++consumed;
     }
     // final store layout must keep the lanes on tile bits 0..4
-    bool low_in_regs = false;
-    for (int b : cur)
-        if (b < lowlanes) low_in_regs = true;
-    if (low_in_regs) {
-        make_stage(load_layout, a.st[ns]);
+    const uint32_t last = stage_bits.empty() ? 0u : stage_bits.back();
+    if (last & lanemask) {
+        uint32_t bits = 0;
+        for (int b = K - 1, c = 0; b >= lowlanes && c < R; --b, ++c) bits |= 1u << b;
+        make_stage(bits, a.st[ns]);
         a.st[ns].op_begin = uint16_t(nops);
         a.st[ns].op_count = 0;
         ++ns;
@@ -1079,19 +1126,25 @@ int build_reg(const qs_pass& ps, const qs_op* ops, int first, int n, int R, int 
     a.nstages = ns;
     a.nops = nops;
     a.nmats = moff;
-    return consumed;
+    std::vector<int> left;
+    for (int i = 0; i < m; ++i)
+        if (!has(done, i)) left.push_back(rem[i]);
+    rem.swap(left);
+    return ndone;
 }
 
 template <typename V, int R>
 int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
     static thread_local RegArgs args;
     config_smem((const void*)k_fused_reg<V, R>);
-    int first = 0;
-    while (first < ps.op_count) {
+    std::vector<int> rem(ps.op_count);
+    for (int i = 0; i < ps.op_count; ++i) rem[i] = i;
+    while (!rem.empty()) {
         // bank-group bits of a shared-memory phase: 8 x 16-byte or 16 x 8-byte elements
-        int used = build_reg(ps, ops, first, n, R, sizeof(V) == 16 ? 3 : 4, args);
+        const int next = ps.op_begin + rem.front();
+        int used = build_reg(ps, ops, rem, n, R, sizeof(V) == 16 ? 3 : 4, args);
         if (used <= 0) {
-            set_error("qs_apply_fused: op %d does not fit a register tile", ps.op_begin + first);
+            set_error("qs_apply_fused: op %d does not fit a register tile", next);
             return QS_EINVAL;
         }
         size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
@@ -1100,7 +1153,6 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
         uint64_t cap = uint64_t(sm_count());
         k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), 1 << (ps.k - R), smem, st>>>(vec, args, mats);
         QS_CHECK_LAUNCH("qs_apply_fused(reg)");
-        first += used;
     }
     return QS_OK;
 }
