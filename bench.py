@@ -223,7 +223,7 @@ def _events_ms(fn, reps):
     return a.elapsed_time(b) / reps
 
 
-def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=2):
+def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
     """Device-timed gates/s of the config-1 circuit at n qubits (extra precisions / sizes)."""
     import torch
     from quict_b200 import _native as N
@@ -262,6 +262,7 @@ def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=2):
     torch.cuda.empty_cache()
     return {"workload": f"sv-{n}q-{'c128' if precision == 'double' else 'c64'}-{N_GATES}g-config1",
             "gates_per_s": ws * len(ops) / (ms / 1e3), "ms_per_run": ms, "fused_passes": passes,
+            "knobs": eng.knobs(vec, n).to_json(),
             "state_bytes": (1 << n) * (16 if precision == "double" else 8)}
 
 
@@ -321,6 +322,17 @@ SWEEP_2Q = ("cx", "cz", "rzz", "swap")
 
 
 SECTOR = 32  # bytes: the L2 / DRAM sector, the smallest unit a skipped run can save
+
+
+def knob_source(eng, vec, n):
+    """Where the fused-pass knobs of this run come from."""
+    import torch
+    from quict_b200.simulation.autotune import tune_key
+    explicit = None not in (eng.tile_bits, eng.low_bits, eng.merge_bits, eng.max_pass_cost)
+    if explicit:
+        return "command line"
+    key = tune_key(torch.cuda.get_device_name(eng.device), vec.element_size(), n, eng.tune_kind)
+    return "tuning cache" if eng.tuner.lookup(key) else "defaults (no cache entry)"
 
 
 def sweep_bytes(name, bits, n, esize):
@@ -464,6 +476,7 @@ def run_ours(args, ws, rank, local):
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded config-1 circuit)",
         "config": {"workload": f"sv-{n}q-c128-{N_GATES}g-config1", "qubits": n, "gates": len(ops),
                    "state_bytes": (1 << n) * 16, "fused_passes": npasses, "single_gate_launches": nsingle,
+                   "knobs": eng.knobs(vec, n).to_json(), "knobs_source": knob_source(eng, vec, n),
                    "l2": "inputs larger than L2 (16 GiB state vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "hbm_gbs_effective": npasses * bytes_per_pass / (ms / 1e3) / 1e9,
@@ -506,11 +519,12 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
-    ap.add_argument("--merge-bits", type=int, default=2, help="gate-merging block width (0 disables)")
+    ap.add_argument("--merge-bits", type=int, default=None,
+                    help="gate-merging block width (0 disables; default: the tuning cache)")
     ap.add_argument("--no-extra", action="store_true", help="skip the complex64 30q / 32q runs")
     ap.add_argument("--qaoa-instances", type=int, default=512)
-    ap.add_argument("--max-pass-cost", type=float, default=float("inf"),
-                    help="fusion width: per-pass arithmetic bound in dense-1q-gate units")
+    ap.add_argument("--max-pass-cost", type=float, default=None,
+                    help="fusion width: per-pass arithmetic bound in dense-1q-gate units (default: the tuning cache)")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -68,7 +68,7 @@ def lower_dm(g, n: int, legacy_2q_order: bool = False) -> List[Op]:
 class DensityMatrixSimulator:
     def __init__(self, device: str = "GPU", precision: str = "double", accumulated_mode: bool = False, *,
                  gpu_device_id: int = 0, fusion: bool = True, tile_bits: Optional[int] = None,
-                 low_bits: Optional[int] = None, merge_bits: int = 2, seed=None):
+                 low_bits: Optional[int] = None, merge_bits: Optional[int] = None, seed=None):
         if device != "GPU":
             raise ValueError(f"DensityMatrixSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
         if precision not in ("single", "double"):
@@ -78,7 +78,7 @@ class DensityMatrixSimulator:
         self._accumulated_mode = accumulated_mode
         self._tdev = require_cuda(gpu_device_id)
         self._engine = Engine(self._tdev, fusion=fusion, tile_bits=tile_bits, low_bits=low_bits,
-                              merge_bits=merge_bits)
+                              merge_bits=merge_bits, tune_kind="dm")
         self._rng = seed if hasattr(seed, "random") else np.random.default_rng(seed)
         self._density_matrix: Optional[torch.Tensor] = None
         self._circuit = None

@@ -13,7 +13,8 @@ import numpy as np
 import torch
 
 from .. import _native as N
-from .fusion import MatrixTable, Pass, Single, default_tile, emit, fusable, plan
+from .autotune import Autotuner, Knobs, default_knobs, tune_key
+from .fusion import MatrixTable, Pass, Single, emit, fusable, plan
 from .lowering import Op
 
 DTYPES = {
@@ -52,14 +53,21 @@ class Workspace:
 
 
 class Engine:
+    """Fused-pass knobs left as None are resolved per (dtype, qubit count) from
+    the autotuner's cache (``autotune.Autotuner``), else from its defaults."""
+
     def __init__(self, device: torch.device, fusion: bool = True, tile_bits: Optional[int] = None,
-                 low_bits: Optional[int] = None, max_pass_cost: float = float("inf"), merge_bits: int = 2):
+                 low_bits: Optional[int] = None, max_pass_cost: Optional[float] = None,
+                 merge_bits: Optional[int] = None, tune_kind: str = "sv", tuner: Optional[Autotuner] = None):
         self.device = device
         self.merge_bits = merge_bits
         self.fusion = fusion
         self.tile_bits = tile_bits
         self.low_bits = low_bits
         self.max_pass_cost = max_pass_cost
+        self.tune_kind = tune_kind
+        self.tuner = tuner or Autotuner()
+        self._resolved = {}  # (element size, n) -> Knobs from the cache / defaults
         self.ws = Workspace(device)
         self.launches = 0  # libqsim kernel launches issued (per gate or per fused pass)
         self.h2d_bytes = 0  # host->device bytes copied for matrix tables
@@ -96,13 +104,36 @@ class Engine:
         self.launches += 1
 
     # ---- fused path -------------------------------------------------------------------
-    def tile_shape(self, vec: torch.Tensor):
-        k0, l0 = default_tile(vec.element_size())
-        return (self.tile_bits or k0), (self.low_bits if self.low_bits is not None else l0)
+    def knobs(self, vec: torch.Tensor, n: int) -> Knobs:
+        """Knobs for a run on `vec` (n qubits): explicit settings win, the rest
+        come from the tuning cache for this GPU, dtype and size."""
+        esize = vec.element_size()
+        kn = self._resolved.get((esize, n))
+        if kn is None:
+            kn = self.tuner.lookup(tune_key(torch.cuda.get_device_name(self.device), esize, n, self.tune_kind))
+            kn = kn or default_knobs(esize)
+            self._resolved[(esize, n)] = kn
+        return Knobs(self.tile_bits if self.tile_bits is not None else kn.tile_bits,
+                     self.low_bits if self.low_bits is not None else kn.low_bits,
+                     self.merge_bits if self.merge_bits is not None else kn.merge_bits,
+                     self.max_pass_cost if self.max_pass_cost is not None else kn.max_pass_cost)
+
+    def tile_shape(self, vec: torch.Tensor, n: int):
+        kn = self.knobs(vec, n)
+        return kn.tile_bits, kn.low_bits
 
     def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
-        k, nlow = self.tile_shape(vec)
-        return plan(ops, n, k, nlow, max_cost=self.max_pass_cost, merge_bits=self.merge_bits)
+        kn = self.knobs(vec, n)
+        return plan(ops, n, kn.tile_bits, kn.low_bits, max_cost=kn.max_pass_cost, merge_bits=kn.merge_bits)
+
+    def autotune(self, vec: torch.Tensor, n: int, ops: Sequence[Op], force: bool = False):
+        """Tune the knobs on `ops` (overwrites `vec`) unless the cache already
+        has an entry for this GPU / dtype / size; returns the knobs in use."""
+        key = tune_key(torch.cuda.get_device_name(self.device), vec.element_size(), n, self.tune_kind)
+        if force or self.tuner.lookup(key) is None:
+            self.tuner.tune(self, vec, n, ops, kind=self.tune_kind)
+        self._resolved.pop((vec.element_size(), n), None)
+        return self.knobs(vec, n)
 
     def run_passes(self, vec: torch.Tensor, n: int, passes: List[Pass]):
         if not passes:

@@ -69,8 +69,8 @@ class StateVectorSimulator:
     def __init__(self, device: str = "GPU", precision: str = "double", gpu_device_id: int = 0,
                  matrix_aggregation: bool = True, sync: bool = True, *, fusion: bool = True,
                  tile_bits: Optional[int] = None, low_bits: Optional[int] = None,
-                 max_pass_cost: float = float("inf"), merge_bits: int = 2, legacy_2q_order: bool = False,
-                 seed: Optional[int] = None):
+                 max_pass_cost: Optional[float] = None, merge_bits: Optional[int] = None,
+                 legacy_2q_order: bool = False, seed: Optional[int] = None, autotune: bool = False):
         if device not in self.__DEVICE:
             raise ValueError(f"StateVectorSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
         if precision not in self.__PRECISION:
@@ -83,8 +83,11 @@ class StateVectorSimulator:
         self._using_matrix_aggregation = matrix_aggregation
         self._legacy = legacy_2q_order
         self._tdev = require_cuda(gpu_device_id)
+        # fused-pass knobs left as None come from the tuning cache; with
+        # autotune=True a run whose size has no cache entry tunes them first
         self._engine = Engine(self._tdev, fusion=fusion, tile_bits=tile_bits, low_bits=low_bits,
                               max_pass_cost=max_pass_cost, merge_bits=merge_bits)
+        self._autotune = autotune
         # measurement uniforms: a seed, or any object with a .random() method
         self._rng = seed if hasattr(seed, "random") else np.random.default_rng(seed)
         self._circuit = None
@@ -150,6 +153,11 @@ class StateVectorSimulator:
                 raise ValueError("The state vector should have the same qubits as the circuit.")
             self._vector = sv.clone() if isinstance(state_vector, (torch.Tensor, StateArray)) else sv
         elif not use_previous or self._vector is None or self._vector.numel() != (1 << n):
+            if self._autotune and self._engine.fusion:
+                self._vector = torch.empty(1 << n, dtype=self._tdtype, device=self._tdev)
+                ops = [op for g in circuit.gates if not _is_trigger(g)
+                       for op in lower_gate(g, n, self._legacy) if op.kind not in ("measure", "reset", "perm")]
+                self._engine.autotune(self._vector, n, ops)
             self.initial_state_vector()
         self._run_gates(list(circuit.gates))
         if self._sync:
