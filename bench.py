@@ -525,7 +525,7 @@ def run_ours(args, ws, rank, local):
         "config": {"workload": f"sv-{n}q-c128-{N_GATES}g-config1", "qubits": n, "gates": len(ops),
                    "state_bytes": (1 << n) * 16, "fused_passes": npasses, "single_gate_launches": nsingle,
                    "knobs": eng.knobs(vec, n).to_json(), "knobs_source": knob_source(eng, vec, n),
-                   "l2": "inputs larger than L2 (16 GiB state vs 126 MB L2)",
+                   "l2": f"inputs larger than L2 ({(1 << n) * 16 / 2**30:g} GiB state vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "hbm_gbs_effective": npasses * bytes_per_pass / (ms / 1e3) / 1e9,
         "roofline": {"bound": "fp64", "kernel": "k_fused_reg", "achieved": fp64_achieved, "peak": fp64_peak,
