@@ -671,22 +671,28 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     KStage* sst = reinterpret_cast<KStage*>((reinterpret_cast<uintptr_t>(sops + p.nops) + 15) & ~uintptr_t(15));
     for (int o = threadIdx.x; o < p.nops; o += blockDim.x) sops[o] = p.ops[o];
     for (int o = threadIdx.x; o < p.nstages; o += blockDim.x) sst[o] = p.st[o];
-    // stage the pass's matrices in slot order (per instance when batched)
+    // stage the pass's matrices in slot order (per instance when batched):
+    // one entry per thread and step over all ops' entries, so the loads of a
+    // restage are independent; `eop` maps an entry to its op
+    uint8_t* eop = reinterpret_cast<uint8_t*>(sst + p.nstages);
+    for (int o = 0; o < p.nops; ++o) {
+        const KCopy& c = p.cp[o];
+        const int cnt = c.diag ? (1 << c.m) : (1 << (2 * c.m));
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) eop[c.soff + e] = uint8_t(o);
+    }
+    __syncthreads();
     auto stage_mats = [&](uint64_t inst) {
-        for (int o = 0; o < p.nops; ++o) {
-            const KCopy& c = p.cp[o];
+        for (int g = threadIdx.x; g < p.nmats; g += blockDim.x) {
+            const KCopy& c = p.cp[eop[g]];
+            const int e = g - c.soff;
             const int D = 1 << c.m;
-            const int cnt = c.diag ? D : D * D;
-            const V* src = mats + c.goff + int64_t(inst) * c.stride;
-            for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-                const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
-                int sr = 0, sc = 0;
-                for (int i = 0; i < c.m; ++i) {
-                    sr |= ((kr >> i) & 1) << c.perm[i];
-                    sc |= ((kc >> i) & 1) << c.perm[i];
-                }
-                msm[c.soff + e] = src[c.diag ? sr : sr * D + sc];
+            const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
+            int sr = 0, sc = 0;
+            for (int i = 0; i < c.m; ++i) {
+                sr |= ((kr >> i) & 1) << c.perm[i];
+                sc |= ((kc >> i) & 1) << c.perm[i];
             }
+            msm[g] = mats[c.goff + int64_t(inst) * c.stride + (c.diag ? sr : sr * D + sc)];
         }
     };
     uint64_t staged = 0;
@@ -715,14 +721,27 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
         for (int t = 0; t < H; ++t) b = insert0(b, p.hi[t]);
         return b;
     };
-    uint64_t tile = blockIdx.x;
-    if (tile < ntiles) tile_prefetch<V>(bufs[0], vec, tile_base(tile), K, L, hoff);
-    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    // tile order: strided over the grid; batched passes take contiguous runs
+    // of tiles instead, so that a CTA restages per-instance matrices once per
+    // instance rather than once per tile
+    uint64_t tile, tend, tstep;
+    if (p.batched) {
+        const uint64_t chunk = (ntiles + gridDim.x - 1) / gridDim.x;
+        tile = uint64_t(blockIdx.x) * chunk;
+        tend = tile + chunk < ntiles ? tile + chunk : ntiles;
+        tstep = 1;
+    } else {
+        tile = blockIdx.x;
+        tend = ntiles;
+        tstep = gridDim.x;
+    }
+    if (tile < tend) tile_prefetch<V>(bufs[0], vec, tile_base(tile), K, L, hoff);
+    for (int it = 0; tile < tend; ++it, tile += tstep) {
         V* cur = bufs[it & 1];
         const uint64_t base = tile_base(tile);
         cp_async_wait_all();
         __syncthreads();  // tile landed; the other buffer is free; previous tile's ops are done
-        if (tile + gridDim.x < ntiles) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + gridDim.x), K, L, hoff);
+        if (tile + tstep < tend) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + tstep), K, L, hoff);
         if (p.batched) {
             const uint64_t inst = base >> p.inst_shift;
             if (inst != staged) {
@@ -1148,10 +1167,16 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
             return QS_EINVAL;
         }
         size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
-                      sizeof(KOp) * args.nops + 16 + sizeof(KStage) * args.nstages;
+                      sizeof(KOp) * args.nops + 16 + sizeof(KStage) * args.nstages + args.nmats;
         uint64_t ntiles = uint64_t(1) << (n - ps.k);
-        uint64_t cap = uint64_t(sm_count());
-        k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), 1 << (ps.k - R), smem, st>>>(vec, args, mats);
+        // persistent grid: as many CTAs as fit on the SMs at once (smaller
+        // tiles run several CTAs per SM, whose relayouts and arithmetic overlap)
+        const int threads = 1 << (ps.k - R);
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_reg<V, R>, threads, smem);
+        if (occ < 1) occ = 1;
+        uint64_t cap = uint64_t(sm_count()) * uint64_t(occ);
+        k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), threads, smem, st>>>(vec, args, mats);
         QS_CHECK_LAUNCH("qs_apply_fused(reg)");
     }
     return QS_OK;
@@ -1165,7 +1190,7 @@ int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
     constexpr int R = reg_bits<V>();
     const int nT = ps.k - R;
     const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
-                        sizeof(KOp) * QS_MAX_PASS_OPS + 16 + sizeof(KStage) * kMaxStages;
+                        sizeof(KOp) * QS_MAX_PASS_OPS + 16 + sizeof(KStage) * kMaxStages + QS_MAX_PASS_MATS;
     if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
     return launch_smem<V, false>(vec, nullptr, n, ps, ops, mats, nullptr, st);
 }
