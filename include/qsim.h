@@ -97,8 +97,12 @@ typedef struct qs_op {
 /* One fused pass: a tile of 2^k amplitudes made of vector bits 0..nlow-1 and
  * hi[0..k-nlow-1] (ascending), and ops [op_begin, op_begin+op_count).
  * Batched state (inst_shift > 0): the vector holds instances of 2^inst_shift
- * amplitudes; instance = index >> inst_shift.  All tile bits must be below
- * inst_shift, so a tile belongs to one instance. */
+ * amplitudes; instance = index >> inst_shift (with the pair bit cleared).
+ * All tile bits other than the pair bit must be below inst_shift, so a tile
+ * belongs to one instance.
+ * pair: 0, or b + 1 where vector bit b separates psi (0) from lam (1) in the
+ * combined vector of qs_adjoint_pair; b must be a tile bit of every pass
+ * that has EXPECT ops. */
 typedef struct qs_pass {
     int32_t k;
     int32_t nlow;
@@ -106,7 +110,7 @@ typedef struct qs_pass {
     int32_t op_begin;
     int32_t op_count;
     int32_t inst_shift;
-    int32_t pad;
+    int32_t pair;
 } qs_pass;
 
 /* ---- library ------------------------------------------------------------ */
@@ -171,6 +175,19 @@ int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes, int npass
 int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs_pass* passes, int npasses,
                      const qs_op* ops, int64_t nops_total, const void* mats_dev, int64_t mats_count,
                      double* partials_dev, int64_t partials_count, void* stream);
+
+/* The same backward sweep on ONE vector of 2^n amplitudes holding psi in the
+ * half where bit b = pair - 1 is 0 and lam in the other half (every pass sets
+ * `pair`, and passes with EXPECT ops keep bit b in their tile; with
+ * instances, b is the top bit).  Ops
+ * on the other bits act on both halves at once, and the register-tile kernel
+ * keeps each psi amplitude beside its lam partner, so EXPECT ops run on chip
+ * between the gates.  partials: as for qs_adjoint_fused, ntiles = 2^(n - k).
+ * Needs register tiles: k in [9, 12] (complex128) or [10, 13] (complex64),
+ * nlow >= 5.  Replaces the same per-parameter re-runs as qs_adjoint_fused. */
+int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* passes, int npasses,
+                    const qs_op* ops, int64_t nops_total, const void* mats_dev, int64_t mats_count,
+                    double* partials_dev, int64_t partials_count, void* stream);
 
 /* out = sum_t c_t P_t psi for Pauli strings P_t = i^popc(x&z) X^x Z^z (x, z:
  * HOST arrays of masks over vector bits, coeff: HOST complex128 pairs).  out

@@ -65,7 +65,7 @@ class qs_pass(C.Structure):
         ("op_begin", C.c_int32),
         ("op_count", C.c_int32),
         ("inst_shift", C.c_int32),
-        ("pad", C.c_int32),
+        ("pair", C.c_int32),
     ]
 
 
@@ -89,6 +89,7 @@ SIGNATURES = {
     "qs_apply_fused": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp]),
     "qs_adjoint_fused": (_i, [_vp, _vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp,
                               _i64, _vp]),
+    "qs_adjoint_pair": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _i64, _vp, _i64, _vp]),
     "qs_apply_pauli_sum": (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp]),
     "qs_inner_batched": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp, _sz, _vp]),
     "qs_segment_sum": (_i, [_vp, _i64, _i64, _vp, _vp]),

@@ -320,7 +320,7 @@ struct KOp {
     uint16_t moff;    // shared-memory offset of the slot-ordered matrix
     uint8_t flags;
     uint8_t ns;       // DIAG: number of slot targets
-    uint8_t pad[2];
+    uint16_t elocal;  // EXPECT: index of the op's partial among the pass's EXPECT ops
     uint64_t gctrl;   // control mask on vector bits outside the tile
     uint8_t kidx[32]; // DIAG: slot s -> index of its slot bits in the diagonal
 };
@@ -346,7 +346,10 @@ struct __align__(16) KStage {
 };
 struct RegArgs {
     int n, K, L, H, nT, nstages, nops, nmats, inst_shift, batched;
+    int nexp;           // EXPECT ops (adjoint pair passes)
+    uint64_t pairmask;  // vector bit separating psi / lam (adjoint pair passes), else 0
     int hi[QS_MAX_TILE_BITS];
+    int eslot[QS_MAX_PASS_OPS];  // output slot of each EXPECT op
     KStage st[kMaxStages];
     KOp ops[QS_MAX_PASS_OPS];
     KCopy cp[QS_MAX_PASS_OPS];
@@ -522,13 +525,51 @@ __device__ __forceinline__ void r_diag_any(V (&x)[E], const V* __restrict__ Dm, 
     }
 }
 
+// ---- EXPECT ops (adjoint pair passes): slot bit 0 holds the psi/lam pair bit,
+// so x[s] (bit 0 clear) is a psi amplitude and x[s | 1] its lam partner.
+// Adds sum conj(lam) (G psi) over the thread's amplitudes to (re, im) in FP64.
+template <typename V, int E, int MASK>
+__device__ __forceinline__ void r_expect_dense(const V (&x)[E], const V* __restrict__ Gm, double& re, double& im) {
+    constexpr int D = 1 << popc_c(MASK);
+    sfor<E>([&](auto sc) __attribute__((always_inline)) {
+        constexpr int s = decltype(sc)::value;
+        if constexpr ((s & MASK) == 0 && (s & 1) == 0) {
+            sfor<D>([&](auto rc) __attribute__((always_inline)) {
+                constexpr int r = decltype(rc)::value;
+                V acc = cmul(Gm[r * D], x[s]);
+                sfor<D - 1>([&](auto cc) __attribute__((always_inline)) {
+                    constexpr int c = decltype(cc)::value + 1;
+                    acc = cfma(Gm[r * D + c], x[s | pdep_c(c, MASK)], acc);
+                });
+                const V l = x[s | 1 | pdep_c(r, MASK)];
+                re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
+                im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+            });
+        }
+    });
+}
+
+template <typename V, int E>
+__device__ __forceinline__ void r_expect_diag(const V (&x)[E], const V* __restrict__ Dm, uint32_t h, const KOp& op,
+                                              double& re, double& im) {
+    const V* d = Dm + (h << op.ns);
+#pragma unroll
+    for (int s = 0; s < E; s += 2) {
+        const V acc = cmul(d[op.kidx[s]], x[s]);
+        const V l = x[s | 1];
+        re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
+        im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+    }
+}
+
 #define QS_MASKS_1_31(F)                                                                             \
     F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15) F(16) F(17) \
         F(18) F(19) F(20) F(21) F(22) F(23) F(24) F(25) F(26) F(27) F(28) F(29) F(30) F(31)
 
-template <typename V, int R>
+template <typename V, int R, bool EXP>
 __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* __restrict__ msm, uint32_t thr,
-                                        uint64_t base, V* __restrict__ buf, const Addr<R>& ad) {
+                                        uint64_t base, V* __restrict__ buf, const Addr<R>& ad,
+                                        double2* __restrict__ ered) {
     constexpr int E = 1 << R;
     const V* Mm = msm + op.moff;
     const uint32_t scm = op.scm;
@@ -568,6 +609,36 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
         break;
                 QS_MASKS_1_31(QS_CASE)
 #undef QS_CASE
+            }
+            break;
+        case QS_OP_EXPECT:
+            if constexpr (EXP) {
+                double re = 0.0, im = 0.0;
+                if (op.flags & QS_OPF_DIAG) {
+                    uint32_t h = 0;
+                    for (int q = 0; q < op.nh; ++q) {
+                        const int src = op.hsrc[q];
+                        const uint32_t bit = src < 64 ? (thr >> src) & 1u : uint32_t((base >> (src - 64)) & 1u);
+                        h = (h << 1) | bit;
+                    }
+                    r_expect_diag<V, E>(x, Mm, h, op, re, im);
+                } else {
+                    switch (op.mask) {
+#define QS_CASE(MK)                                                                           \
+    case MK:                                                                                  \
+        if constexpr ((MK) < (1 << R) && ((MK) & 1) == 0 && popc_c(MK) <= 2) r_expect_dense<V, E, MK>(x, Mm, re, im); \
+        break;
+                        QS_MASKS_1_31(QS_CASE)
+#undef QS_CASE
+                    }
+                }
+                // warp sum in a fixed order; lane 0 records the warp's partial
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    re += __shfl_xor_sync(0xffffffffu, re, off);
+                    im += __shfl_xor_sync(0xffffffffu, im, off);
+                }
+                if ((threadIdx.x & 31) == 0) ered[op.elocal * (blockDim.x >> 5) + (threadIdx.x >> 5)] = make_double2(re, im);
             }
             break;
         default: {  // QS_OP_DIAG
@@ -655,9 +726,11 @@ __device__ __forceinline__ void tile_prefetch(V* __restrict__ dst, const V* __re
     cp_async_commit();
 }
 
-template <typename V, int R>
+// EXP: adjoint pair pass (psi and lam halves in one vector, EXPECT ops write
+// per-tile partials to `partials`).
+template <typename V, int R, bool EXP>
 __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const __grid_constant__ RegArgs p,
-                                                      const V* __restrict__ mats) {
+                                                      const V* __restrict__ mats, double* __restrict__ partials) {
     constexpr int E = 1 << R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = p.K, L = p.L, H = p.H, nT = p.nT;
@@ -675,6 +748,8 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     // one entry per thread and step over all ops' entries, so the loads of a
     // restage are independent; `eop` maps an entry to its op
     uint8_t* eop = reinterpret_cast<uint8_t*>(sst + p.nstages);
+    // EXPECT partials of the current tile: [EXPECT op][warp]
+    double2* ered = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(eop + p.nmats) + 15) & ~uintptr_t(15));
     for (int o = 0; o < p.nops; ++o) {
         const KCopy& c = p.cp[o];
         const int cnt = c.diag ? (1 << c.m) : (1 << (2 * c.m));
@@ -743,7 +818,7 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
         __syncthreads();  // tile landed; the other buffer is free; previous tile's ops are done
         if (tile + tstep < tend) tile_prefetch<V>(bufs[(it + 1) & 1], vec, tile_base(tile + tstep), K, L, hoff);
         if (p.batched) {
-            const uint64_t inst = base >> p.inst_shift;
+            const uint64_t inst = (base & ~p.pairmask) >> p.inst_shift;
             if (inst != staged) {
                 stage_mats(inst);
                 staged = inst;
@@ -766,7 +841,7 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
                 const KOp& op = sops[o];
                 if ((base & op.gctrl) != op.gctrl) continue;
                 if ((thr & op.tctrl) != op.tctrl) continue;
-                r_apply<V, R>(x, op, msm, thr, base, cur, ad);
+                r_apply<V, R, EXP>(x, op, msm, thr, base, cur, ad, ered);
             }
         }
         {  // registers -> global in the last stage's layout (lanes on tile bits 0..4)
@@ -775,6 +850,20 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
                 constexpr int s = decltype(sc)::value;
                 vec[b0 | gslot_store[s]] = x[s];
             });
+        }
+        if constexpr (EXP) {  // per-tile partials: warp partials summed in a fixed order
+            __syncthreads();
+            const int nw = blockDim.x >> 5;
+            for (int e = threadIdx.x; e < p.nexp; e += blockDim.x) {
+                double2 t = make_double2(0.0, 0.0);
+                for (int w = 0; w < nw; ++w) {
+                    t.x += ered[e * nw + w].x;
+                    t.y += ered[e * nw + w].y;
+                }
+                const uint64_t at = 2 * (uint64_t(p.eslot[e]) * ntiles + tile);
+                partials[at] = t.x;
+                partials[at + 1] = t.y;
+            }
         }
     }
 }
@@ -796,9 +885,14 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
         tilemask |= uint64_t(1) << ps.hi[t];
     }
     QS_REQUIRE(ps.inst_shift >= 0 && ps.inst_shift <= n, "inst_shift %d outside [0, n]", ps.inst_shift);
+    QS_REQUIRE(ps.pair >= 0 && ps.pair <= n, "pair %d outside [0, n]", ps.pair);
+    QS_REQUIRE(ps.pair == 0 || adjoint, "pair bits belong to adjoint pair passes");
+    const uint64_t pairmask = ps.pair > 0 ? uint64_t(1) << (ps.pair - 1) : 0;
+    QS_REQUIRE(ps.pair == 0 || ps.inst_shift == 0 || ps.pair == n, "with instances, the pair bit must be the top bit");
     if (ps.inst_shift > 0)
-        QS_REQUIRE((tilemask >> ps.inst_shift) == 0, "tile bits must lie below inst_shift (one instance per tile)");
-    const int64_t ninst = ps.inst_shift > 0 ? (int64_t(1) << (n - ps.inst_shift)) : 1;
+        QS_REQUIRE(((tilemask & ~pairmask) >> ps.inst_shift) == 0,
+                   "tile bits must lie below inst_shift (one instance per tile)");
+    const int64_t ninst = ps.inst_shift > 0 ? (int64_t(1) << (n - ps.inst_shift - (ps.pair > 0 ? 1 : 0))) : 1;
     const int64_t ntiles = int64_t(1) << (n - ps.k);
     int local[64];
     for (int b = 0; b < 64; ++b) local[b] = -1;
@@ -814,6 +908,7 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
             QS_REQUIRE(op.m <= 2 || (op.flags & QS_OPF_DIAG), "op %d: dense EXPECT generators act on <= 2 bits", i);
             QS_REQUIRE(op.slot >= 0 && (int64_t(op.slot) + 1) * ntiles * 2 <= partials_count,
                        "op %d: EXPECT slot %d outside the partials buffer", i, op.slot);
+            QS_REQUIRE(ps.pair == 0 || (tilemask & pairmask), "op %d: EXPECT needs the pair bit in the tile", i);
         }
         QS_REQUIRE(op.m >= 1 && op.m <= 4, "op %d: m=%d outside [1, 4]", i, op.m);
         QS_REQUIRE(op.kind != QS_OP_ANTI || op.m == 1, "op %d: ANTI needs m = 1", i);
@@ -840,6 +935,14 @@ int validate_pass(const qs_pass& ps, int n, const qs_op* ops, int64_t nops_total
     return QS_OK;
 }
 
+// Largest dynamic shared memory a block may opt into on the current device.
+int smem_optin() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v > 0 ? v : 200 * 1024;
+}
+
 // Opt a kernel into large dynamic shared memory once per (kernel, device).
 void config_smem(const void* fn) {
     static thread_local std::vector<std::pair<const void*, int>> done;
@@ -847,7 +950,10 @@ void config_smem(const void* fn) {
     cudaGetDevice(&dev);
     for (const auto& d : done)
         if (d.first == fn && d.second == dev) return;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    // the opt-in limit covers static and dynamic shared memory together
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, fn);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin() - int(fa.sharedSizeBytes));
     done.emplace_back(fn, dev);
 }
 
@@ -946,14 +1052,28 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     a.n = n; a.K = K; a.L = L; a.H = K - L; a.nT = nT;
     a.inst_shift = ps.inst_shift;
     a.batched = 0;
+    a.nexp = 0;
+    a.pairmask = ps.pair > 0 ? uint64_t(1) << (ps.pair - 1) : 0;
     for (int t = 0; t < QS_MAX_TILE_BITS; ++t) a.hi[t] = t < K - L ? ps.hi[t] : 0;
+    // tile position of the psi/lam pair bit (adjoint pair passes): EXPECT ops
+    // need it in registers, where it always takes slot bit 0
+    int pair_tile = -1;
+    if (ps.pair > 0) {
+        if (ps.pair - 1 < L) pair_tile = ps.pair - 1;
+        for (int t = 0; t < K - L; ++t)
+            if (ps.hi[t] == ps.pair - 1) pair_tile = L + t;
+    }
     const int lowlanes = 5;  // tile bits 0..4 are the lanes of the load/store layout
     const uint32_t lanemask = (1u << lowlanes) - 1u;
     auto make_stage = [&](uint32_t bits, KStage& S) {
         int j = 0, i = 0;
+        if (pair_tile >= 0 && ((bits >> pair_tile) & 1)) S.R[j++] = uint8_t(pair_tile);
         for (int b = 0; b < K; ++b) {
-            if ((bits >> b) & 1) S.R[j++] = uint8_t(b);
-            else S.T[i++] = uint8_t(b);
+            if ((bits >> b) & 1) {
+                if (b != pair_tile) S.R[j++] = uint8_t(b);
+            } else {
+                S.T[i++] = uint8_t(b);
+            }
         }
         for (; j < 6; ++j) S.R[j] = 0;
         for (; i < 8; ++i) S.T[i] = 0;
@@ -961,20 +1081,24 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     // ---- dependency graph
     const int m = int(rem.size());
     using Set = std::array<uint64_t, (QS_MAX_PASS_OPS + 63) / 64>;
-    std::vector<uint32_t> xm(m), am(m);
+    std::vector<uint32_t> xm(m), am(m), need(m);  // dense bits, all bits, bits needed in registers
     std::vector<int> msz(m);
     std::vector<Set> pred(m);
     for (int i = 0; i < m; ++i) {
         const qs_op& op = ops[ps.op_begin + rem[i]];
+        const bool dg = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
         uint32_t x = 0, all = op.lctrl;
         for (int j = 0; j < op.m; ++j)
             if (op.tgt[j] >= 0) {
                 all |= 1u << op.tgt[j];
-                if (op.kind != QS_OP_DIAG) x |= 1u << op.tgt[j];
+                if (!dg) x |= 1u << op.tgt[j];
             }
         xm[i] = x;
         am[i] = all;
-        msz[i] = op.kind == QS_OP_DIAG ? (1 << op.m) : (1 << (2 * op.m));
+        // EXPECT ops read psi/lam pairs: the pair bit must be in registers (no
+        // other op touches it, so it adds no ordering)
+        need[i] = x | (op.kind == QS_OP_EXPECT && pair_tile >= 0 ? 1u << pair_tile : 0u);
+        msz[i] = dg ? (1 << op.m) : (1 << (2 * op.m));
         pred[i].fill(0);
         for (int h = 0; h < i; ++h)
             if ((xm[h] & am[i]) | (am[h] & xm[i])) pred[i][h >> 6] |= uint64_t(1) << (h & 63);
@@ -990,7 +1114,7 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     auto score = [&](uint32_t bits, Set d) {
         int c = 0;
         for (int i = 0; i < m; ++i)
-            if (!has(d, i) && !(xm[i] & ~bits) && ready(d, i)) {
+            if (!has(d, i) && !(need[i] & ~bits) && ready(d, i)) {
                 d[i >> 6] |= uint64_t(1) << (i & 63);
                 ++c;
             }
@@ -1020,7 +1144,7 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
         if (best_score < 0) break;
         std::vector<int> order;
         for (int i = 0; i < m; ++i)
-            if (!has(done, i) && !(xm[i] & ~best) && ready(done, i)) {
+            if (!has(done, i) && !(need[i] & ~best) && ready(done, i)) {
                 if (mats + msz[i] > QS_MAX_PASS_MATS) {
                     full = true;
                     continue;
@@ -1075,7 +1199,11 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
             if (op.mat_stride != 0) a.batched = 1;
             c.soff = uint16_t(moff);
             c.m = uint8_t(op.m);
-            c.diag = op.kind == QS_OP_DIAG;
+            c.diag = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+            if (op.kind == QS_OP_EXPECT) {
+                k.elocal = uint16_t(a.nexp);
+                a.eslot[a.nexp++] = op.slot;
+            }
             k.moff = uint16_t(moff);
             // slot-ordered bit permutation
             int slots[4], js[4], ns_ = 0;
@@ -1152,10 +1280,10 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     return ndone;
 }
 
-template <typename V, int R>
-int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+template <typename V, int R, bool EXP>
+int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
     static thread_local RegArgs args;
-    config_smem((const void*)k_fused_reg<V, R>);
+    config_smem((const void*)k_fused_reg<V, R, EXP>);
     std::vector<int> rem(ps.op_count);
     for (int i = 0; i < ps.op_count; ++i) rem[i] = i;
     while (!rem.empty()) {
@@ -1166,18 +1294,23 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
             set_error("qs_apply_fused: op %d does not fit a register tile", next);
             return QS_EINVAL;
         }
+        const int threads = 1 << (ps.k - R);
         size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
-                      sizeof(KOp) * args.nops + 16 + sizeof(KStage) * args.nstages + args.nmats;
+                      sizeof(KOp) * args.nops + 16 + sizeof(KStage) * args.nstages + args.nmats +
+                      (EXP ? 16 + sizeof(double2) * size_t(args.nexp) * (threads / 32) : 0);
+        if (smem > size_t(smem_optin())) {
+            set_error("qs_apply_fused: a register pass needs %zu bytes of shared memory", smem);
+            return QS_EINVAL;
+        }
         uint64_t ntiles = uint64_t(1) << (n - ps.k);
         // persistent grid: as many CTAs as fit on the SMs at once (smaller
         // tiles run several CTAs per SM, whose relayouts and arithmetic overlap)
-        const int threads = 1 << (ps.k - R);
         int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_reg<V, R>, threads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_reg<V, R, EXP>, threads, smem);
         if (occ < 1) occ = 1;
         uint64_t cap = uint64_t(sm_count()) * uint64_t(occ);
-        k_fused_reg<V, R><<<unsigned(ntiles < cap ? ntiles : cap), threads, smem, st>>>(vec, args, mats);
-        QS_CHECK_LAUNCH("qs_apply_fused(reg)");
+        k_fused_reg<V, R, EXP><<<unsigned(ntiles < cap ? ntiles : cap), threads, smem, st>>>(vec, args, mats, partials);
+        QS_CHECK_LAUNCH(EXP ? "qs_adjoint_pair" : "qs_apply_fused(reg)");
     }
     return QS_OK;
 }
@@ -1191,7 +1324,8 @@ int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
     const int nT = ps.k - R;
     const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
                         sizeof(KOp) * QS_MAX_PASS_OPS + 16 + sizeof(KStage) * kMaxStages + QS_MAX_PASS_MATS;
-    if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= 200 * 1024) return launch_reg<V, R>(vec, n, ps, ops, mats, st);
+    if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= size_t(smem_optin()))
+        return launch_reg<V, R, false>(vec, n, ps, ops, mats, nullptr, st);
     return launch_smem<V, false>(vec, nullptr, n, ps, ops, mats, nullptr, st);
 }
 
@@ -1250,6 +1384,39 @@ extern "C" int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs
                                                   (const double2*)mats_dev, partials_dev, as_stream(stream))
                      : launch_smem<float2, true>((float2*)psi, (float2*)lam, n, passes[i], ops,
                                                  (const float2*)mats_dev, partials_dev, as_stream(stream));
+        if (rc) return rc;
+    }
+    return QS_OK;
+}
+
+extern "C" int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* passes, int npasses, const qs_op* ops,
+                               int64_t nops_total, const void* mats_dev, int64_t mats_count, double* partials_dev,
+                               int64_t partials_count, void* stream) {
+    QS_REQUIRE(psilam != nullptr, "null vector");
+    QS_REQUIRE(n >= 2 && n <= 41, "bit count %d outside [2, 41]", n);
+    QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
+    QS_REQUIRE(npasses >= 0 && (npasses == 0 || passes != nullptr), "bad pass array");
+    QS_REQUIRE(nops_total >= 0 && (nops_total == 0 || ops != nullptr), "bad op array");
+    QS_REQUIRE(mats_count >= 0 && (mats_count == 0 || mats_dev != nullptr), "bad matrix table");
+    QS_REQUIRE(partials_count >= 0 && (partials_count == 0 || partials_dev != nullptr), "bad partials buffer");
+    const int R = dtype == QS_C128 ? reg_bits<double2>() : reg_bits<float2>();
+    for (int i = 0; i < npasses; ++i) {
+        int rc = validate_pass(passes[i], n, ops, nops_total, mats_count, true, partials_count);
+        if (rc) return rc;
+        QS_REQUIRE(passes[i].pair > 0, "pass %d: no pair bit", i);
+        const int nT = passes[i].k - R;
+        QS_REQUIRE(nT >= 5 && nT <= 8 && passes[i].nlow >= 5, "pass %d: tile 2^%d / nlow %d is not a register tile", i,
+                   passes[i].k, passes[i].nlow);
+    }
+    for (int i = 0; i < npasses; ++i) {
+        if (passes[i].op_count == 0) continue;
+        int rc = dtype == QS_C128
+                     ? launch_reg<double2, reg_bits<double2>(), true>((double2*)psilam, n, passes[i], ops,
+                                                                      (const double2*)mats_dev, partials_dev,
+                                                                      as_stream(stream))
+                     : launch_reg<float2, reg_bits<float2>(), true>((float2*)psilam, n, passes[i], ops,
+                                                                    (const float2*)mats_dev, partials_dev,
+                                                                    as_stream(stream));
         if (rc) return rc;
     }
     return QS_OK;

@@ -9,10 +9,16 @@ so a fused pass advances every instance at once.
   forward   psi = U(theta)|0>                       (fused passes, qs_apply_fused)
             lam = H psi                             (qs_apply_pauli_sum)
             E   = <psi|lam> per instance            (qs_inner_batched, FP64)
-  backward  for gates k = L..1 (fused into tile passes, qs_adjoint_fused):
+  backward  for gates k = L..1 (fused into tile passes, qs_adjoint_pair):
               g_k += scale_k * Im <lam| G_k |psi>   (per-tile FP64 partials)
               psi <- U_k^dagger psi,  lam <- U_k^dagger lam
             partials -> per (gate, instance) sums   (qs_segment_sum)
+
+psi and lam live in the two halves of one vector; the top bit (the "pair
+bit") selects the half.  The backward passes run on that vector with the pair
+bit in the tile, so the register-tile kernel holds each psi amplitude beside
+its lam partner and applies U^dagger to both with one op.  Instances too small
+for register tiles use the shared-memory kernel (qs_adjoint_fused) instead.
 
 With U(theta) = exp(-i theta G / 2), dE/dtheta_k = 2 Re <lam_k| dU_k |psi_{k-1}>
 = scale_k * Im <lam_k| G_k |psi_k>.  ``parameter_shift`` computes the same
@@ -58,7 +64,7 @@ class BatchedAdjoint:
     """Energies and gradients of <psi(theta)|H|psi(theta)> for a batch of theta."""
 
     def __init__(self, circuit: ParamCircuit, observable: PauliSum, precision: str = "single",
-                 device_id: int = 0, tile_bits: Optional[int] = None):
+                 device_id: int = 0, tile_bits: Optional[int] = None, pair: bool = True):
         if observable.n != circuit.n:
             raise ValueError("observable and circuit act on different qubit counts")
         self.circuit = circuit
@@ -71,6 +77,11 @@ class BatchedAdjoint:
         # the adjoint pass keeps two tiles (psi, lam) on chip
         self.k = min(tile_bits or (k0 - 1), self.n)
         self.nlow = min(5, self.k)
+        # register-tile backward on the psi/lam pair vector: tile of k0 bits,
+        # one of them the pair bit; needs 2^(R+5) <= tile (R = 4 / 5)
+        self.pair_k = min(k0, self.n + 1)
+        self.pair_min_k = 9 if precision == "double" else 10
+        self.pair = pair and self.pair_k >= self.pair_min_k
         self.ws = Workspace(self.dev)
         self.launches = 0
         self.pauli = observable.masks()
@@ -181,11 +192,25 @@ class BatchedAdjoint:
                 ops.append(Op("expect", op.tbits, (), GENERATORS[ent.kind], tag=("expect", entry),
                               slot=slot_of[entry]))
             ops.append(op)
-        gp.bwd = self._build(nbits, ops, adjoint=True)
         gp.nslots = max(1, len(self._param_entries))
-        gp.psi = torch.empty(bp << self.n, dtype=self.cdtype, device=self.dev)
-        gp.lam = torch.empty_like(gp.psi)
-        gp.partials = torch.empty(2 * gp.nslots * (1 << (nbits - self.k)), dtype=torch.float64, device=self.dev)
+        half = bp << self.n
+        # with several instances the tile's non-pair bits must stay below the
+        # instance bits, so the tile takes at most n of them
+        pk = self.pair_k if bp == 1 else min(self.pair_k, self.n)
+        gp.pair = self.pair and pk >= self.pair_min_k
+        if gp.pair:
+            ops = [Op(o.kind, o.tbits, o.cbits, o.mat, tag=o.tag, batch=o.batch, slot=o.slot, extra=(nbits,))
+                   if o.kind == "expect" else o for o in ops]
+            gp.bwd = self._build(nbits + 1, ops, adjoint=True, k=pk, pair=nbits)
+            gp.pl = torch.empty(2 * half, dtype=self.cdtype, device=self.dev)
+            gp.psi, gp.lam = gp.pl[:half], gp.pl[half:]
+            gp.tiles_per_inst = 1 << (self.n + 1 - pk)
+        else:
+            gp.bwd = self._build(nbits, ops, adjoint=True)
+            gp.psi = torch.empty(half, dtype=self.cdtype, device=self.dev)
+            gp.lam = torch.empty_like(gp.psi)
+            gp.tiles_per_inst = 1 << (self.n - self.k)
+        gp.partials = torch.empty(2 * gp.nslots * bp * gp.tiles_per_inst, dtype=torch.float64, device=self.dev)
         gp.sums = torch.empty(2 * gp.nslots * bp, dtype=torch.float64, device=self.dev)
         gp.e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
         gp.ws = torch.empty(16 * bp * 64 + 256, dtype=torch.uint8, device=self.dev)
@@ -198,13 +223,14 @@ class BatchedAdjoint:
         gp.grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
         return gp
 
-    def _build(self, nbits: int, ops: Sequence[Op], adjoint: bool):
-        steps = plan(ops, nbits, self.k, self.nlow, merge_bits=0 if adjoint else 2)
+    def _build(self, nbits: int, ops: Sequence[Op], adjoint: bool, k: Optional[int] = None,
+               pair: Optional[int] = None):
+        steps = plan(ops, nbits, k or self.k, self.nlow, merge_bits=0 if adjoint else 2)
         passes = [s for s in steps if isinstance(s, Pass)]
         if len(passes) != len(steps):
             raise RuntimeError("a gradient-circuit op could not be fused")
         table = MatrixTable()
-        cps, npass, cops, nops = emit(passes, table, inst_shift=self.n)
+        cps, npass, cops, nops = emit(passes, table, inst_shift=self.n, pair=pair)
         mats = torch.from_numpy(table.array().astype(self.np_dtype)).to(self.dev)
         return (cps, npass, cops, nops, mats)
 
@@ -226,10 +252,15 @@ class BatchedAdjoint:
         N.call("qs_inner_batched", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits, qs_dtype(psi),
                n, C.c_void_p(gp.e.data_ptr()), C.c_void_p(gp.ws.data_ptr()), gp.ws.numel(), st)
         cps, npass2, cops, nops, mats = gp.bwd
-        N.call("qs_adjoint_fused", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
-               qs_dtype(psi), cps, npass2, cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
-               C.c_void_p(gp.partials.data_ptr()), int(gp.partials.numel()), st)
-        N.call("qs_segment_sum", C.c_void_p(gp.partials.data_ptr()), gp.nslots * bp, 1 << (n - self.k),
+        if gp.pair:
+            N.call("qs_adjoint_pair", C.c_void_p(gp.pl.data_ptr()), nbits + 1, qs_dtype(psi), cps, npass2, cops,
+                   nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
+                   C.c_void_p(gp.partials.data_ptr()), int(gp.partials.numel()), st)
+        else:
+            N.call("qs_adjoint_fused", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
+                   qs_dtype(psi), cps, npass2, cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
+                   C.c_void_p(gp.partials.data_ptr()), int(gp.partials.numel()), st)
+        N.call("qs_segment_sum", C.c_void_p(gp.partials.data_ptr()), gp.nslots * bp, gp.tiles_per_inst,
                C.c_void_p(gp.sums.data_ptr()), st)
         self.launches += npass + npass2 + 3
         im = gp.sums.view(gp.nslots, bp, 2)[:, :, 1]

@@ -20,7 +20,7 @@ The reference has no counterpart: it launches one kernel per gate
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Dict, List, Sequence, Tuple, Union
+from typing import Dict, List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -100,8 +100,9 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
                 stop = True
                 continue
             xb, zb = op.xbits, op.zbits
-            allb = xb | zb
-            hoistable = not (allb & xblk) and not (xb & zblk)
+            xc = xb - frozenset(op.extra)  # extra bits are tile requirements, not conflicts
+            allb = xc | zb
+            hoistable = not (allb & xblk) and not (xc & zblk)
             need = xb - low - hi
             c = op_cost(op)
             ent = op_entries(op)
@@ -113,7 +114,7 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
                 entries += ent
             else:
                 deferred.append(op)
-                xblk |= xb
+                xblk |= xc
                 zblk |= zb
         # fill unused tile bits with the lowest free bits (longer contiguous runs)
         b = nlow
@@ -270,10 +271,11 @@ class MatrixTable:
         return np.concatenate(self._chunks)
 
 
-def emit(passes: Sequence[Pass], table: MatrixTable, inst_shift: int = 0):
+def emit(passes: Sequence[Pass], table: MatrixTable, inst_shift: int = 0, pair: Optional[int] = None):
     """Convert passes into ctypes (qs_pass[], qs_op[]) arrays, filling `table`.
     inst_shift > 0 marks a batched state (instance = index >> inst_shift); ops
-    with per-instance tables (``Op.batch``) then get a matrix stride."""
+    with per-instance tables (``Op.batch``) then get a matrix stride.  `pair`:
+    the vector bit separating psi from lam in an adjoint pair vector."""
     cps = (N.qs_pass * max(1, len(passes)))()
     nops = sum(len(p.ops) for p in passes)
     cops = (N.qs_op * max(1, nops))()
@@ -285,6 +287,7 @@ def emit(passes: Sequence[Pass], table: MatrixTable, inst_shift: int = 0):
             cp.hi[j] = h
         cp.op_begin, cp.op_count = o, len(p.ops)
         cp.inst_shift = inst_shift
+        cp.pair = 0 if pair is None else pair + 1
         local = {b: b for b in range(p.nlow)}
         for j, h in enumerate(p.hi):
             local[h] = p.nlow + j

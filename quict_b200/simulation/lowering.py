@@ -36,6 +36,7 @@ class Op:
     tag: object = None            # caller data (e.g. parameter index for gradients); blocks merging
     batch: Optional[np.ndarray] = None  # per-instance tables, shape (instances, entries)
     slot: int = -1                # "expect": output slot
+    extra: Tuple[int, ...] = ()   # further bits the op needs in its tile (e.g. the psi/lam pair bit)
 
     @property
     def m(self) -> int:
@@ -49,8 +50,8 @@ class Op:
     def xbits(self) -> frozenset:
         """Bits on which the op is not diagonal (must be tile-resident when fused)."""
         if self.kind in ("mat", "antidiag", "swap") or (self.kind == "expect" and not self.is_diag_expect):
-            return frozenset(self.tbits)
-        return frozenset()
+            return frozenset(self.tbits) | frozenset(self.extra)
+        return frozenset(self.extra)
 
     @property
     def zbits(self) -> frozenset:

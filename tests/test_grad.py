@@ -174,3 +174,36 @@ def test_uneven_qaoa_graph_vs_per_instance_c128(cuda_ok):
     torch.cuda.synchronize()
     for (e, g), (e3, g3) in zip(res, batch.results()):
         assert e == e3 and np.array_equal(g, g3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("double", 1e-10), ("single", 1e-4)])
+def test_pair_vector_backward_matches_shared_memory_path(cuda_ok, precision, tol):
+    """The register-tile backward on the psi/lam pair vector (qs_adjoint_pair)
+    against the shared-memory backward (qs_adjoint_fused) and the FP64 oracle's
+    parameter shift, for a batch (pair bit above the instance bits) and for one
+    QAOA instance (pair bit just above the qubits)."""
+    from quict_b200.differentiation import BatchedAdjoint, maxcut_observable, qaoa_circuit, random_regular_graph
+    n = 10
+    circ, obs = _hea(n, 2)
+    params = np.random.default_rng(4).uniform(0, 2 * np.pi, (4, circ.num_params))
+    fast = BatchedAdjoint(circ, obs, precision)
+    slow = BatchedAdjoint(circ, obs, precision, pair=False)
+    gp = fast.plan_gradient(params)
+    assert gp.pair and not slow.plan_gradient(params).pair
+    e1, g1 = fast.gradient(params)
+    e2, g2 = slow.gradient(params)
+    np.testing.assert_allclose(e1.cpu().numpy(), e2.cpu().numpy(), atol=tol)
+    np.testing.assert_allclose(g1.cpu().numpy(), g2.cpu().numpy(), atol=tol)
+    fn, h = _matrices_fn(circ), obs.matrix()
+    want = oobs.param_shift(fn, params[1], n, h, _occurrences(circ))
+    np.testing.assert_allclose(g1[1].cpu().numpy(), want, atol=tol)
+    edges = random_regular_graph(n, 3, np.random.default_rng(2))
+    qc, qo = qaoa_circuit(n, edges, 2), maxcut_observable(n, edges)
+    prm = np.random.default_rng(5).uniform(0, 3, (1, qc.num_params))
+    a, b = BatchedAdjoint(qc, qo, precision), BatchedAdjoint(qc, qo, precision, pair=False)
+    assert a.plan_gradient(prm).pair
+    ea, ga = a.gradient(prm)
+    eb, gb = b.gradient(prm)
+    assert abs(float(ea[0]) - float(eb[0])) < tol * len(edges)
+    np.testing.assert_allclose(ga.cpu().numpy(), gb.cpu().numpy(), atol=tol * len(edges))
