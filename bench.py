@@ -13,8 +13,10 @@ value   gates/s with the state resident in HBM, device-timed (CUDA events),
 e2e     the same metric through the public API (StateVectorSimulator.run):
         host planning, matrix-table host->device copy and a device->host read
         of P(qubit 0 = 0) inside every step.
-roofline  the fused-pass kernel (k_fused): algorithmic bytes 2 * 2^n * 16 per
-        launch over its CUDA-event duration, against MEASURED_PEAKS.json.
+roofline  the fused-pass kernel (k_fused_reg), bound fp64: algorithmic flops of
+        its ops over its CUDA-event time, against cuBLAS DGEMM measured here;
+        roofline_hbm: 2 * 2^n * 16 bytes per launch against MEASURED_PEAKS.json.
+single_gate_sweep, c64, adjoint, qaoa  extra sections.
 cpu_baseline  the numba port of the reference CPU kernels (oracle/ref_port.py)
         on this host's cores, on the first gates of the same circuit.
 """
@@ -258,11 +260,12 @@ def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
     barrier(ws)
     ms = max_over_ranks(_events_ms(step, steps), ws)
     passes = sum(1 for s in plan_ if isinstance(s, Pass) and s.ops)
+    knobs = eng.knobs(vec, n).to_json()
     del sim, vec
     torch.cuda.empty_cache()
     return {"workload": f"sv-{n}q-{'c128' if precision == 'double' else 'c64'}-{N_GATES}g-config1",
             "gates_per_s": ws * len(ops) / (ms / 1e3), "ms_per_run": ms, "fused_passes": passes,
-            "knobs": eng.knobs(vec, n).to_json(),
+            "knobs": knobs,
             "state_bytes": (1 << n) * (16 if precision == "double" else 8)}
 
 
