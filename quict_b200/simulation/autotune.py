@@ -31,9 +31,9 @@ from typing import Callable, Dict, List, Optional, Sequence
 PACKAGED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
 
 # register-kernel tile widths per element size: 2^R amplitudes per thread and
-# 32..256 threads per tile (tile_bits = R + 5 .. R + 8); k = R + 8 is the
-# full-block default
-_TILE_CHOICES = {16: (11, 12), 8: (12, 13)}
+# 64..256 threads per tile (tile_bits = R + 6 .. R + 8); narrower tiles run
+# several CTAs per SM.  k = R + 8 is the default when the cache has no entry.
+_TILE_CHOICES = {16: (10, 11, 12), 8: (11, 12, 13)}
 
 
 @dataclass(frozen=True)

@@ -17,12 +17,13 @@ def test_knobs_json_round_trip():
 
 
 def test_candidates_respect_register_tile_widths():
-    for esize, ks in ((16, {11, 12}), (8, {12, 13})):
+    for esize, ks in ((16, {10, 11, 12}), (8, {11, 12, 13})):
         c = candidates(esize, 30)
         assert {kn.tile_bits for kn in c} == ks
         assert {kn.merge_bits for kn in c} == {0, 2, 3}
         assert default_knobs(esize).tile_bits == max(ks)
     assert all(kn.tile_bits <= 11 for kn in candidates(16, 11))
+    assert len(candidates(16, 30)) == 18
 
 
 def test_cache_precedence_user_over_packaged(tmp_path):
