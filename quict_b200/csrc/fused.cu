@@ -527,10 +527,14 @@ __device__ __forceinline__ void r_diag_any(V (&x)[E], const V* __restrict__ Dm, 
 
 // ---- EXPECT ops (adjoint pair passes): slot bit 0 holds the psi/lam pair bit,
 // so x[s] (bit 0 clear) is a psi amplitude and x[s | 1] its lam partner.
-// Adds sum conj(lam) (G psi) over the thread's amplitudes to (re, im) in FP64.
+// Adds sum conj(lam) (G psi) over the thread's amplitudes to (re, im): the
+// thread's few products are summed in the state's precision (one conversion
+// per op instead of one per product) and everything above that in FP64.
 template <typename V, int E, int MASK>
 __device__ __forceinline__ void r_expect_dense(const V (&x)[E], const V* __restrict__ Gm, double& re, double& im) {
+    using S = decltype(V::x);
     constexpr int D = 1 << popc_c(MASK);
+    S pr = 0, pi = 0;
     sfor<E>([&](auto sc) __attribute__((always_inline)) {
         constexpr int s = decltype(sc)::value;
         if constexpr ((s & MASK) == 0 && (s & 1) == 0) {
@@ -542,24 +546,30 @@ __device__ __forceinline__ void r_expect_dense(const V (&x)[E], const V* __restr
                     acc = cfma(Gm[r * D + c], x[s | pdep_c(c, MASK)], acc);
                 });
                 const V l = x[s | 1 | pdep_c(r, MASK)];
-                re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
-                im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+                pr += l.x * acc.x + l.y * acc.y;
+                pi += l.x * acc.y - l.y * acc.x;
             });
         }
     });
+    re += double(pr);
+    im += double(pi);
 }
 
 template <typename V, int E>
 __device__ __forceinline__ void r_expect_diag(const V (&x)[E], const V* __restrict__ Dm, uint32_t h, const KOp& op,
                                               double& re, double& im) {
+    using S = decltype(V::x);
     const V* d = Dm + (h << op.ns);
+    S pr = 0, pi = 0;
 #pragma unroll
     for (int s = 0; s < E; s += 2) {
         const V acc = cmul(d[op.kidx[s]], x[s]);
         const V l = x[s | 1];
-        re += double(l.x) * double(acc.x) + double(l.y) * double(acc.y);
-        im += double(l.x) * double(acc.y) - double(l.y) * double(acc.x);
+        pr += l.x * acc.x + l.y * acc.y;
+        pi += l.x * acc.y - l.y * acc.x;
     }
+    re += double(pr);
+    im += double(pi);
 }
 
 #define QS_MASKS_1_31(F)                                                                             \
@@ -638,7 +648,7 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
                     re += __shfl_xor_sync(0xffffffffu, re, off);
                     im += __shfl_xor_sync(0xffffffffu, im, off);
                 }
-                if ((threadIdx.x & 31) == 0) ered[op.elocal * (blockDim.x >> 5) + (threadIdx.x >> 5)] = make_double2(re, im);
+                if ((threadIdx.x & 31) == 0) ered[op.elocal] = make_double2(re, im);  // this warp's row
             }
             break;
         default: {  // QS_OP_DIAG
@@ -748,8 +758,9 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
     // one entry per thread and step over all ops' entries, so the loads of a
     // restage are independent; `eop` maps an entry to its op
     uint8_t* eop = reinterpret_cast<uint8_t*>(sst + p.nstages);
-    // EXPECT partials of the current tile: [EXPECT op][warp]
+    // EXPECT partials of the current tile: [warp][EXPECT op]; ered_w is this warp's row
     double2* ered = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(eop + p.nmats) + 15) & ~uintptr_t(15));
+    double2* ered_w = ered + (threadIdx.x >> 5) * p.nexp;
     for (int o = 0; o < p.nops; ++o) {
         const KCopy& c = p.cp[o];
         const int cnt = c.diag ? (1 << c.m) : (1 << (2 * c.m));
@@ -841,7 +852,7 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
                 const KOp& op = sops[o];
                 if ((base & op.gctrl) != op.gctrl) continue;
                 if ((thr & op.tctrl) != op.tctrl) continue;
-                r_apply<V, R, EXP>(x, op, msm, thr, base, cur, ad, ered);
+                r_apply<V, R, EXP>(x, op, msm, thr, base, cur, ad, ered_w);
             }
         }
         {  // registers -> global in the last stage's layout (lanes on tile bits 0..4)
@@ -857,8 +868,8 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
             for (int e = threadIdx.x; e < p.nexp; e += blockDim.x) {
                 double2 t = make_double2(0.0, 0.0);
                 for (int w = 0; w < nw; ++w) {
-                    t.x += ered[e * nw + w].x;
-                    t.y += ered[e * nw + w].y;
+                    t.x += ered[w * p.nexp + e].x;
+                    t.y += ered[w * p.nexp + e].y;
                 }
                 const uint64_t at = 2 * (uint64_t(p.eslot[e]) * ntiles + tile);
                 partials[at] = t.x;
