@@ -65,3 +65,32 @@ def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int =
     obs = ising_observable(n)
     params = np.random.default_rng(seed).uniform(0, 2 * np.pi, (batch, circ.num_params))
     return circ, obs, params
+
+
+def main() -> None:
+    """Run one workload on cuda:0 (for profiling a single kernel family):
+
+        python -m quict_b200.workloads gradient --batch 256 [--precision single] [--repeat 2]
+    """
+    import argparse
+
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", choices=["gradient"])
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--precision", default="single", choices=["single", "double"])
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args()
+    from .differentiation import BatchedAdjoint
+    circ, obs, params = config3_problem(16, 8, a.batch)
+    eng = BatchedAdjoint(circ, obs, a.precision)
+    gp = eng.plan_gradient(params)
+    for _ in range(a.repeat):
+        eng.launch(gp)
+    torch.cuda.synchronize()
+    print(f"gradient batch {a.batch} {a.precision}: |grad|_1 = {float(gp.gradients.abs().sum()):.6e}")
+
+
+if __name__ == "__main__":
+    main()
