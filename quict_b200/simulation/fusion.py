@@ -134,6 +134,17 @@ def _embed(u: np.ndarray, bits: Tuple[int, ...], into: Tuple[int, ...]) -> np.nd
     k, m = len(into), len(bits)
     if tuple(bits) == tuple(into):
         return u
+    if k == 2 and m == 1:  # the common merge step, written out (np.kron dominates planning time)
+        t = np.zeros((2, 2, 2, 2), dtype=np.complex128)
+        if bits[0] == into[0]:
+            t[:, 0, :, 0] = u
+            t[:, 1, :, 1] = u
+        else:
+            t[0, :, 0, :] = u
+            t[1, :, 1, :] = u
+        return t.reshape(4, 4)
+    if m == 0:
+        return np.eye(1 << k, dtype=np.complex128) * u.reshape(())
     full = np.kron(u, np.eye(1 << (k - m), dtype=np.complex128))  # order: bits, then the rest
     order = list(bits) + [b for b in into if b not in bits]
     # permute tensor axes from `order` to `into`
