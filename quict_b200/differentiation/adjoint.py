@@ -47,17 +47,87 @@ def _pow2(b: int) -> int:
     return p
 
 
-def _batched_rotations(kind: str, thetas: np.ndarray, inverse: bool = False) -> Tuple[str, np.ndarray]:
-    """Per-instance exp(-i t G/2) tables: ("diag", (B, 2^m)) or ("mat", (B, 4^m))."""
-    g = GENERATORS[kind]
+def _batched_rotations(kind, thetas: np.ndarray, inverse: bool = False) -> Tuple[str, np.ndarray]:
+    """Per-instance exp(-i t G/2) tables: ("diag", (B, 2^m)) or ("mat", (B, 4^m)).
+    `kind`: a GENERATORS key or a generator matrix (diagonal ones may have any
+    real eigenvalues; dense ones must square to I)."""
+    g = GENERATORS[kind] if isinstance(kind, str) else kind
     t = -thetas if inverse else thetas
+    if classify(g) == "diag":
+        return "diag", np.exp(-0.5j * t[:, None] * np.diag(g).real[None, :])
     c = np.cos(t / 2)[:, None]
     s = np.sin(t / 2)[:, None]
-    if classify(g) == "diag":
-        d = np.diag(g)[None, :]
-        return "diag", c - 1j * s * d
     eye = np.eye(g.shape[0]).ravel()[None, :]
     return "mat", c * eye - 1j * s * g.ravel()[None, :]
+
+
+class _Unit:
+    """One op of the gradient circuit: a fixed gate, a parameterised gate, or a
+    group of commuting diagonal gates sharing one parameter (e.g. the Rzz gates
+    of a QAOA cost layer) merged into one diagonal on at most 4 qubits."""
+
+    def __init__(self, entries: List[int], qubits: Tuple[int, ...], gen: Optional[np.ndarray] = None,
+                 fixed: Optional[np.ndarray] = None, index: int = -1, scale: float = 1.0):
+        self.entries, self.qubits, self.gen, self.fixed = entries, qubits, gen, fixed
+        self.index, self.scale = index, scale
+
+
+def _diag_on(g: np.ndarray, qubits: Sequence[int], into: Sequence[int]) -> np.ndarray:
+    """Diagonal of generator g (on `qubits`, big-endian) as a diagonal on `into`."""
+    d = np.diag(g).real
+    k = len(into)
+    out = np.zeros(1 << k)
+    for idx in range(1 << k):
+        sub = 0
+        for q in qubits:
+            sub = (sub << 1) | ((idx >> (k - 1 - into.index(q))) & 1)
+        out[idx] = d[sub]
+    return out
+
+
+def gate_units(circuit: ParamCircuit, cluster: bool = True, max_qubits: int = 4) -> List[_Unit]:
+    """The circuit as gate units.  With `cluster`, each maximal run of
+    consecutive diagonal rotations with the same parameter and scale (they
+    commute) is split greedily into groups of at most `max_qubits` qubits, and
+    each group becomes one diagonal unit whose generator is the sum of the
+    group's generators; its gradient term then covers the whole group."""
+    E = circuit.entries
+    out: List[_Unit] = []
+    i = 0
+    while i < len(E):
+        e = E[i]
+        if e.kind == "fixed":
+            out.append(_Unit([i], e.qubits, fixed=e.matrix))
+            i += 1
+            continue
+        g = GENERATORS[e.kind]
+        j = i + 1
+        if cluster and classify(g) == "diag":
+            while (j < len(E) and E[j].kind != "fixed" and classify(GENERATORS[E[j].kind]) == "diag"
+                   and E[j].index == e.index and E[j].scale == e.scale):
+                j += 1
+        if j - i == 1:
+            out.append(_Unit([i], e.qubits, gen=g, index=e.index, scale=e.scale))
+            i = j
+            continue
+        groups: List[Tuple[set, List[int]]] = []
+        for t in range(i, j):
+            qs = set(E[t].qubits)
+            best, shared = None, -1
+            for grp in groups:
+                if len(grp[0] | qs) <= max_qubits and len(grp[0] & qs) > shared:
+                    best, shared = grp, len(grp[0] & qs)
+            if best is None:
+                groups.append((set(qs), [t]))
+            else:
+                best[0].update(qs)
+                best[1].append(t)
+        for qs, members in groups:
+            into = tuple(sorted(qs))
+            d = sum(_diag_on(GENERATORS[E[t].kind], E[t].qubits, into) for t in members)
+            out.append(_Unit(members, into, gen=np.diag(d).astype(np.complex128), index=e.index, scale=e.scale))
+        i = j
+    return out
 
 
 class BatchedAdjoint:
@@ -86,6 +156,9 @@ class BatchedAdjoint:
         self.launches = 0
         self.pauli = observable.masks()
         self._param_entries = [i for i, e in enumerate(circuit.entries) if e.kind != "fixed"]
+        self._units = gate_units(circuit, cluster=True)        # forward / adjoint sweep
+        self._units_plain = gate_units(circuit, cluster=False)  # one unit per entry (parameter shift)
+        self._param_units = [u for u, un in enumerate(self._units) if un.fixed is None]
 
     # ---- helpers ---------------------------------------------------------------------------
     @property
@@ -95,17 +168,18 @@ class BatchedAdjoint:
     def _vbits(self, qubits: Sequence[int]) -> Tuple[int, ...]:
         return tuple(self.n - 1 - q for q in qubits)
 
-    def _gate_ops(self, params: np.ndarray, inverse: bool) -> List[Tuple[int, Op]]:
-        """[(entry index, op)] in circuit order; per-instance tables for rotations."""
+    def _gate_ops(self, params: np.ndarray, inverse: bool, units: Optional[List[_Unit]] = None
+                  ) -> List[Tuple[int, Op]]:
+        """[(unit index, op)] in circuit order; per-instance tables for rotations."""
         out = []
-        for i, e in enumerate(self.circuit.entries):
-            tb = self._vbits(e.qubits)
-            if e.kind == "fixed":
-                m = np.conj(e.matrix.T) if inverse else e.matrix
+        for i, u in enumerate(self._units if units is None else units):
+            tb = self._vbits(u.qubits)
+            if u.fixed is not None:
+                m = np.conj(u.fixed.T) if inverse else u.fixed
                 k = classify(m)
                 out.append((i, Op("diag", tb, (), np.diag(m).copy()) if k == "diag" else Op(k, tb, (), m.copy())))
             else:
-                kind, tab = _batched_rotations(e.kind, e.scale * params[:, e.index], inverse)
+                kind, tab = _batched_rotations(u.gen, u.scale * params[:, u.index], inverse)
                 m0 = tab[0].copy() if kind == "diag" else tab[0].reshape(1 << len(tb), -1)
                 out.append((i, Op(kind, tb, (), m0, tag=("param", i), batch=tab)))
         return out
@@ -184,15 +258,14 @@ class BatchedAdjoint:
         gp = GradientPlan(b=b, bp=bp, nbits=nbits)
         gp.fwd = self._build(nbits, [op for _, op in self._gate_ops(p, False)], adjoint=False)
         inv = self._gate_ops(p, True)
-        slot_of = {entry: s for s, entry in enumerate(self._param_entries)}
+        slot_of = {u: s for s, u in enumerate(self._param_units)}
         ops: List[Op] = []
-        for entry, op in reversed(inv):
-            ent = self.circuit.entries[entry]
-            if ent.kind != "fixed":
-                ops.append(Op("expect", op.tbits, (), GENERATORS[ent.kind], tag=("expect", entry),
-                              slot=slot_of[entry]))
+        for ui, op in reversed(inv):
+            un = self._units[ui]
+            if un.fixed is None:
+                ops.append(Op("expect", op.tbits, (), un.gen, tag=("expect", ui), slot=slot_of[ui]))
             ops.append(op)
-        gp.nslots = max(1, len(self._param_entries))
+        gp.nslots = max(1, len(self._param_units))
         half = bp << self.n
         # with several instances the tile's non-pair bits must stay below the
         # instance bits, so the tile takes at most n of them
@@ -217,8 +290,8 @@ class BatchedAdjoint:
         # gradient = W @ Im<lam|G|psi>, W[param, slot] = scale: a fixed-order (deterministic)
         # sum over the gates that share a parameter
         w = np.zeros((self.circuit.num_params, gp.nslots))
-        for s_, e in enumerate(self._param_entries):
-            w[self.circuit.entries[e].index, s_] += self.circuit.entries[e].scale
+        for s_, u in enumerate(self._param_units):
+            w[self._units[u].index, s_] += self._units[u].scale
         gp.weights = torch.from_numpy(w).to(self.dev)
         gp.grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
         return gp
@@ -293,7 +366,7 @@ class BatchedAdjoint:
 
     def _shifted_ops(self, p: np.ndarray, entry: int, shift: float) -> List[Op]:
         ops = []
-        for i, op in self._gate_ops(p, False):
+        for i, op in self._gate_ops(p, False, self._units_plain):
             if i == entry:
                 ent = self.circuit.entries[i]
                 kind, tab = _batched_rotations(ent.kind, ent.scale * p[:, ent.index] + shift)

@@ -207,3 +207,28 @@ def test_pair_vector_backward_matches_shared_memory_path(cuda_ok, precision, tol
     eb, gb = b.gradient(prm)
     assert abs(float(ea[0]) - float(eb[0])) < tol * len(edges)
     np.testing.assert_allclose(ga.cpu().numpy(), gb.cpu().numpy(), atol=tol * len(edges))
+
+
+def test_qaoa_cost_layer_units_match_the_gates():
+    """Commuting Rzz gates that share a parameter are grouped into diagonal units
+    of at most 4 qubits; the units' product equals the gates' product."""
+    from quict_b200.differentiation import maxcut_observable, qaoa_circuit, random_regular_graph
+    from quict_b200.differentiation.adjoint import _batched_rotations, gate_units
+    n, p = 8, 2
+    edges = random_regular_graph(n, 3, np.random.default_rng(1))
+    circ = qaoa_circuit(n, edges, p)
+    params = np.random.default_rng(2).uniform(0, 3, circ.num_params)
+    units = gate_units(circ)
+    assert len(units) < len(circ.entries)
+    assert all(len(u.qubits) <= 4 for u in units)
+    mats = []
+    for u in units:
+        if u.fixed is not None:
+            mats.append((u.fixed, list(u.qubits)))
+        else:
+            kind, tab = _batched_rotations(u.gen, np.array([u.scale * params[u.index]]))
+            m = np.diag(tab[0]) if kind == "diag" else tab[0].reshape(1 << len(u.qubits), -1)
+            mats.append((m, list(u.qubits)))
+    np.testing.assert_allclose(osv.run(mats, n), osv.run(circ.matrices(params), n), atol=1e-12)
+    plain = gate_units(circ, cluster=False)
+    assert len(plain) == len(circ.entries)
