@@ -320,6 +320,41 @@ def qaoa_bench(ws, rank, local, count=512):
             "launches_per_replay": sum(e.launches for e in batch.engines) // 2}
 
 
+def small_configs_bench(ws, local, reps=3):
+    """Configs 0 and 2 through the public API, wall time per call with the
+    device synchronised on both sides (host planning and copies included):
+    config 0 = StateVectorSimulator.run of the 20-qubit 200-gate circuit, then
+    sample(8192); config 2 = DensityMatrixSimulator.run of the 12-qubit
+    150-gate circuit with composed damping + depolarizing noise per gate."""
+    import torch
+    from quict_b200.simulation import DensityMatrixSimulator, StateVectorSimulator
+    from quict_b200.workloads import config0_circuit, config2_problem
+    dev = torch.device("cuda", local)
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return max_over_ranks((time.perf_counter() - t0) / reps * 1e3, ws)
+
+    c0 = config0_circuit(20, 200, 0)
+    sv = StateVectorSimulator("GPU", "double", gpu_device_id=local)
+    run_ms = wall(lambda: sv.run(c0))
+    sample_ms = wall(lambda: sv.sample(8192, seed=7))
+    c2, nm = config2_problem(12, 150, 2)
+    dm = DensityMatrixSimulator("GPU", "double", accumulated_mode=True, gpu_device_id=local)
+    dm_ms = wall(lambda: dm.run(c2, noise_model=nm))
+    return {"config0": {"workload": "sv-20q-c128-200g-config0 + 8192 shots", "run_ms": run_ms,
+                        "sample_8192_ms": sample_ms, "gates_per_s": ws * 200 / (run_ms / 1e3)},
+            "config2": {"workload": "dm-12q-c128-150g-damping+depolarizing", "run_ms": dm_ms,
+                        "gates_per_s": ws * 150 / (dm_ms / 1e3)},
+            "timing": "wall clock per public call, device synchronised, max over ranks"}
+
+
 SWEEP_1Q = ("h", "x", "rx", "ry", "rz", "u3")
 SWEEP_2Q = ("cx", "cz", "rzz", "swap")
 
@@ -551,6 +586,8 @@ def run_ours(args, ws, rank, local):
     torch.cuda.empty_cache()
     if not args.no_extra:
         line["c64"] = [sv_rate(30, "single", local, ws), sv_rate(32, "single", local, ws)]
+    if not args.no_extra:
+        line["configs_0_2"] = small_configs_bench(ws, local)
     if not args.no_grad:
         line["adjoint"] = grad_bench(ws, rank, local)
         line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances)

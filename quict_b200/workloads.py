@@ -57,6 +57,23 @@ def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: flo
     return c
 
 
+def config2_problem(n: int = 12, size: int = 150, seed: int = 2, gamma: float = 5e-3, p1: float = 1e-3,
+                    p2: float = 1e-2):
+    """Noisy density-matrix run: a `size`-gate circuit from the config-0 gate set,
+    each gate followed by amplitude damping (gamma) composed with depolarizing
+    noise (p1 for 1-qubit gates, p2 for 2-qubit gates) on the touched qubits.
+    Returns (circuit, noise_model)."""
+    from .core import DampingError, DepolarizingError, NoiseModel
+    c = config0_circuit(n, size, seed)
+    one = ["h", "x", "rx", "ry", "rz", "u3"]
+    two = ["cx", "cz", "rzz", "swap"]
+    amp = DampingError(amplitude_prob=gamma, phase_prob=0)
+    nm = NoiseModel(basic_gates=one + two)
+    nm.add_noise_for_all_qubits(amp.compose(DepolarizingError(p1, 1)), one)
+    nm.add_noise_for_all_qubits(amp.tensor(amp).compose(DepolarizingError(p2, 2)), two)
+    return c, nm
+
+
 def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int = 3):
     """Hardware-efficient ansatz (Ry, Rz on every qubit + CZ ring per layer),
     H = sum Z_i Z_{i+1} (open chain) + 0.5 sum X_i, params uniform in [0, 2 pi)."""
