@@ -35,12 +35,10 @@ def _is_noise_gate(g) -> bool:
 
 def superop(kraus: List[np.ndarray]) -> np.ndarray:
     """S = sum_i K_i (x) conj(K_i): (S vec(rho))[(r, c)] = sum K rho K^dagger."""
-    k0 = np.asarray(kraus[0], dtype=np.complex128)
-    s = np.zeros((k0.shape[0] ** 2,) * 2, dtype=np.complex128)
-    for k in kraus:
-        k = np.asarray(k, dtype=np.complex128)
-        s += np.kron(k, np.conj(k))
-    return s
+    k = np.asarray([np.asarray(m, dtype=np.complex128) for m in kraus])
+    d = k.shape[1]
+    # S[(a, c), (b, d)] = sum_i K_i[a, b] conj(K_i[c, d]), all Kraus operators at once
+    return np.einsum("kab,kcd->acbd", k, k.conj()).reshape(d * d, d * d)
 
 
 def lower_dm(g, n: int, legacy_2q_order: bool = False) -> List[Op]:
