@@ -368,7 +368,8 @@ __device__ __forceinline__ void sfor(F&& f) {
 }
 
 // Buffer address of slot s for the current stage: tpos ^ XOR_{j in s} rpos[j].
-// (The swizzle is linear over GF(2), so a swizzled address splits the same way.)
+// (The relayout address maps are linear over GF(2), so a mapped address splits
+// the same way.)
 template <int R>
 struct Addr {
     uint32_t tpos;
@@ -388,7 +389,7 @@ struct Addr {
 // output row goes to this thread's own positions of the tile buffer and is read
 // back after the group.  No other thread reads or writes those positions: the
 // thread holds exactly the amplitudes stored there (plain order in the first
-// stage, swizzled order after a relayout; `ad` addresses whichever applies).
+// stage, the relayout's address map after it; `ad` addresses whichever applies).
 // PRED: some of the op's controls are slot bits (checked per group).
 template <typename V, int E, int R, int MASK, bool PRED>
 __device__ __forceinline__ void r_mat(V (&x)[E], const V* __restrict__ Mm, uint32_t scm, V* __restrict__ buf,
