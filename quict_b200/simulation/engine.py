@@ -14,7 +14,7 @@ import torch
 
 from .. import _native as N
 from .autotune import Autotuner, Knobs, default_knobs, tune_key
-from .fusion import MatrixTable, Pass, Single, emit, fusable, plan
+from .fusion import MatrixTable, Pass, Single, emit, fusable, plan, relabel_swaps
 from .lowering import Op
 
 DTYPES = {
@@ -123,8 +123,11 @@ class Engine:
         return kn.tile_bits, kn.low_bits
 
     def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        """Fused-pass plan of `ops`; plain SWAP gates become relabellings
+        (``fusion.relabel_swaps``), so the plan moves no data for them."""
         kn = self.knobs(vec, n)
-        return plan(ops, n, kn.tile_bits, kn.low_bits, max_cost=kn.max_pass_cost, merge_bits=kn.merge_bits)
+        return plan(relabel_swaps(ops, n), n, kn.tile_bits, kn.low_bits, max_cost=kn.max_pass_cost,
+                    merge_bits=kn.merge_bits)
 
     def autotune(self, vec: torch.Tensor, n: int, ops: Sequence[Op], force: bool = False):
         """Tune the knobs on `ops` (overwrites `vec`) unless the cache already

@@ -59,6 +59,40 @@ def default_tile(dtype_bytes: int) -> Tuple[int, int]:
     return k, nlow
 
 
+def _unit_swap(op: Op) -> bool:
+    m = op.mat
+    return (op.kind == "swap" and not op.cbits and m[0, 0] == 1 and m[1, 2] == 1 and m[2, 1] == 1
+            and m[3, 3] == 1)
+
+
+def relabel_swaps(ops: Sequence[Op], n: int) -> List[Op]:
+    """Turn plain SWAP gates into relabellings: after swap(a, b) every later op
+    addresses the other bit, so the swap moves no data.  At the end a short
+    swap network (at most n - 1 swaps, usually far fewer than were removed)
+    puts every bit back in place.  The result acts exactly like `ops`."""
+    if not any(_unit_swap(op) for op in ops):
+        return list(ops)
+    where = list(range(n))  # logical bit -> physical bit
+    out: List[Op] = []
+    for op in ops:
+        if _unit_swap(op):
+            a, b = op.tbits
+            where[a], where[b] = where[b], where[a]
+            continue
+        out.append(Op(op.kind, tuple(where[b] for b in op.tbits), tuple(where[b] for b in op.cbits), op.mat,
+                      op.perm, op.qubit, op.tag, op.batch, op.slot, op.extra))
+    swap = np.eye(4, dtype=np.complex128)[[0, 2, 1, 3]]
+    holder = {p: q for q, p in enumerate(where)}  # physical bit -> logical bit held
+    for lb in range(n):
+        p = where[lb]
+        if p != lb:
+            other = holder[lb]  # the logical bit sitting where lb belongs
+            out.append(Op("swap", (p, lb), (), swap))
+            where[lb], where[other] = lb, p
+            holder[lb], holder[p] = lb, other
+    return out
+
+
 def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_PASS_OPS,
          max_cost: float = float("inf"), merge_bits: int = 0) -> List[Step]:
     """Greedy in-order planner with commutation-aware hoisting.

@@ -202,3 +202,39 @@ def test_merge_ops_reduces_op_count_and_keeps_kinds():
     ref = _apply_ops_oracle(osv.zero_state(n), n, ops)
     got = _apply_ops_oracle(osv.zero_state(n), n, merged)
     np.testing.assert_allclose(got, ref, atol=1e-13)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_swap_relabelling_acts_like_the_swaps(seed):
+    """Plain SWAP gates become relabellings plus a closing swap network; the
+    rewritten op list gives the same state (FP64 oracle)."""
+    from quict_b200.core import Circuit, Swap
+    from quict_b200.simulation.fusion import relabel_swaps
+    from quict_b200.simulation.lowering import lower_circuit
+    n = 7
+    rng = np.random.default_rng(seed)
+    c = Circuit(n)
+    c.random_append(40, seed=seed)
+    for _ in range(6):
+        a, b = rng.choice(n, 2, replace=False)
+        Swap | c([int(a), int(b)])
+    c.random_append(20, seed=seed + 50)
+    ops = lower_circuit(c.gates, n)
+    new = relabel_swaps(ops, n)
+    assert sum(o.kind == "swap" for o in new) <= sum(o.kind == "swap" for o in ops)
+
+    def run(lst):
+        v = np.zeros(1 << n, dtype=np.complex128)
+        v[0] = 1
+        for op in lst:
+            u = op.dense()
+            bits = tuple(op.cbits) + tuple(op.tbits)
+            if op.cbits:
+                d = u.shape[0] << len(op.cbits)
+                f = np.eye(d, dtype=np.complex128)
+                f[d - u.shape[0]:, d - u.shape[0]:] = u
+                u = f
+            v = osv.apply_matrix(v, n, u, [n - 1 - b for b in bits])
+        return v
+
+    np.testing.assert_allclose(run(new), run(ops), atol=1e-12)
