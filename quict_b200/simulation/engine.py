@@ -14,7 +14,7 @@ import torch
 
 from .. import _native as N
 from .autotune import Autotuner, Knobs, default_knobs, tune_key
-from .fusion import MatrixTable, Pass, Single, emit, fusable, plan, relabel_swaps
+from .fusion import MatrixTable, Pass, Single, emit, fusable, iter_plan, plan, relabel_swaps
 from .lowering import Op
 
 DTYPES = {
@@ -122,12 +122,16 @@ class Engine:
         kn = self.knobs(vec, n)
         return kn.tile_bits, kn.low_bits
 
-    def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
-        """Fused-pass plan of `ops`; plain SWAP gates become relabellings
-        (``fusion.relabel_swaps``), so the plan moves no data for them."""
+    def plan_iter(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        """Fused-pass steps of `ops`, yielded as they are planned; plain SWAP
+        gates become relabellings (``fusion.relabel_swaps``), so the plan moves
+        no data for them."""
         kn = self.knobs(vec, n)
-        return plan(relabel_swaps(ops, n), n, kn.tile_bits, kn.low_bits, max_cost=kn.max_pass_cost,
-                    merge_bits=kn.merge_bits)
+        return iter_plan(relabel_swaps(ops, n), n, kn.tile_bits, kn.low_bits, max_cost=kn.max_pass_cost,
+                         merge_bits=kn.merge_bits)
+
+    def plan(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        return list(self.plan_iter(vec, n, ops))
 
     def autotune(self, vec: torch.Tensor, n: int, ops: Sequence[Op], force: bool = False):
         """Tune the knobs on `ops` (overwrites `vec`) unless the cache already
@@ -144,7 +148,9 @@ class Engine:
         table = MatrixTable()
         cps, npass, cops, nops = emit(passes, table)
         host = table.array().astype(np.complex64 if vec.dtype == torch.complex64 else np.complex128)
-        mats = torch.from_numpy(host).to(self.device)
+        # pinned staging: the copy is queued on the stream without blocking the
+        # host behind kernels already in flight
+        mats = torch.from_numpy(host).pin_memory().to(self.device, non_blocking=True)
         self.h2d_bytes += mats.numel() * mats.element_size()
         if self.pass_events is None:
             N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), cps, npass, cops, nops,
@@ -170,15 +176,13 @@ class Engine:
             for op in ops:
                 self.apply_single(vec, n, op)
             return
-        batch: List[Pass] = []
-        for step in self.plan(vec, n, ops):
+        # each pass is launched as soon as it is planned: the GPU works on it
+        # while the host plans the next one
+        for step in self.plan_iter(vec, n, ops):
             if isinstance(step, Pass):
-                batch.append(step)
+                self.run_passes(vec, n, [step])
             else:
-                self.run_passes(vec, n, batch)
-                batch = []
                 self.apply_single(vec, n, step.op)
-        self.run_passes(vec, n, batch)
 
     # ---- reductions / measurement -------------------------------------------------------
     def prob0(self, src: torch.Tensor, n: int, bit: int, src_kind: int = N.QS_SRC_SV) -> float:

@@ -20,7 +20,7 @@ The reference has no counterpart: it launches one kernel per gate
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Sequence, Tuple, Union
+from typing import Dict, Iterator, List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -95,7 +95,14 @@ def relabel_swaps(ops: Sequence[Op], n: int) -> List[Op]:
 
 def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_PASS_OPS,
          max_cost: float = float("inf"), merge_bits: int = 0) -> List[Step]:
-    """Greedy in-order planner with commutation-aware hoisting.
+    """All steps of ``iter_plan`` as a list."""
+    return list(iter_plan(ops, n, k, nlow, max_ops, max_cost, merge_bits))
+
+
+def iter_plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_PASS_OPS,
+              max_cost: float = float("inf"), merge_bits: int = 0) -> Iterator[Step]:
+    """Greedy in-order planner with commutation-aware hoisting; yields each step
+    as soon as it is final, so a caller can launch it while planning the rest.
 
     ``max_cost`` bounds the per-pass arithmetic, measured in dense-1q-gate
     equivalents (see ``op_cost``), so that a pass stays bandwidth-bound.
@@ -106,7 +113,6 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
     nlow = min(nlow, k)
     H = k - nlow
     low = frozenset(range(nlow))
-    steps: List[Step] = []
     pending = list(ops)
     def fits(op: Op) -> bool:
         return fusable(op) and len(op.xbits - low) <= H
@@ -114,7 +120,7 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
     while pending:
         # leading ops that can never be tile-resident run on their own
         if not fits(pending[0]):
-            steps.append(Single(pending.pop(0)))
+            yield Single(pending.pop(0))
             continue
         hi: set = set()
         chosen: List[Op] = []
@@ -158,9 +164,8 @@ def plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_MAX_P
             b += 1
         if merge_bits > 0:
             chosen = merge_ops(chosen, frozenset(range(nlow)) | frozenset(hi), merge_bits)
-        steps.append(Pass(k, nlow, tuple(sorted(hi)), chosen))
+        yield Pass(k, nlow, tuple(sorted(hi)), chosen)
         pending = deferred
-    return steps
 
 
 def _embed(u: np.ndarray, bits: Tuple[int, ...], into: Tuple[int, ...]) -> np.ndarray:
