@@ -213,9 +213,12 @@ def _to_op(bits: Tuple[int, ...], u: np.ndarray) -> Op:
     return Op(kind, tuple(bits), (), u)
 
 
-def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2) -> List[Op]:
+def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bits: int = 4) -> List[Op]:
     """Multiply runs of ops that act on at most `max_bits` tile-resident bits
-    into single ops (gate fusion at the matrix level).
+    into single ops (gate fusion at the matrix level).  Diagonal ops (phases,
+    Rz, Rzz, CZ, ...) also merge among themselves into diagonal blocks of up to
+    `max_diag_bits` bits on any vector bits: a diagonal costs one complex
+    multiply per amplitude whatever its width.
 
     Open blocks hold disjoint bit sets, so they commute with each other; an op
     that touches several blocks closes them (emits them) first, and an op that
@@ -223,7 +226,7 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2) -> List[Op]
     gradients) closes the blocks it touches and is emitted as is.  Order is
     therefore preserved between every pair of ops that share a bit."""
     out: List[Op] = []
-    blocks: List[list] = []  # [bits tuple, matrix, [source ops]]
+    blocks: List[list] = []  # [bits tuple, matrix, [source ops], all diagonal]
 
     def close(b):
         blocks.remove(b)
@@ -235,36 +238,38 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2) -> List[Op]
     for op in ops:
         S = set(op.tbits) | set(op.cbits)
         hit = [b for b in blocks if S & set(b[0])]
-        mergeable = op.tag is None and S <= tile and len(S) <= max_bits
         union = set(S)
         for b in hit:
             union |= set(b[0])
-        if not mergeable or len(union) > max_bits:
+        diag = op.kind == "diag"
+        free = op.tag is None
+        if free and diag and all(b[3] for b in hit) and len(union) <= max_diag_bits:
+            as_diag = True
+        elif free and union <= tile and len(union) <= max_bits:
+            as_diag = diag and all(b[3] for b in hit)
+        else:
             for b in hit:
                 close(b)
-            if mergeable:
+            if free and ((diag and len(S) <= max_diag_bits) or (S <= tile and len(S) <= max_bits)):
                 bits, u = _full_matrix(op)
-                blocks.append([bits, u, [op]])
+                blocks.append([bits, u, [op], diag])
             else:
                 out.append(op)
             continue
         # merge the hit blocks (disjoint, commuting) and the op into one block
-        if hit:
-            bits: Tuple[int, ...] = ()
-            u = np.eye(1, dtype=np.complex128)
-            srcs: List[Op] = []
-            for b in hit:
-                nb = bits + tuple(x for x in b[0] if x not in bits)
-                u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
-                bits = nb
-                srcs += b[2]
-                blocks.remove(b)
-        else:
-            bits, u, srcs = (), np.eye(1, dtype=np.complex128), []
+        bits: Tuple[int, ...] = ()
+        u = np.eye(1, dtype=np.complex128)
+        srcs: List[Op] = []
+        for b in hit:
+            nb = bits + tuple(x for x in b[0] if x not in bits)
+            u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
+            bits = nb
+            srcs += b[2]
+            blocks.remove(b)
         ob, ou = _full_matrix(op)
         nb = bits + tuple(x for x in ob if x not in bits)
         u = _embed(ou, ob, nb) @ _embed(u, bits, nb)
-        blocks.append([nb, u, srcs + [op]])
+        blocks.append([nb, u, srcs + [op], as_diag])
     for b in list(blocks):
         close(b)
     return out
