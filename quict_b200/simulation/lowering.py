@@ -74,8 +74,18 @@ def _is_controlled(m: np.ndarray, controls: int, targets: int) -> bool:
     if controls == 0:
         return False
     top = m[: d - t, : d - t]
-    return (np.allclose(top, np.eye(d - t), atol=0, rtol=0)
+    return (np.array_equal(top, _eye(d - t))
             and not np.any(m[: d - t, d - t:]) and not np.any(m[d - t:, : d - t]))
+
+
+_EYES = {}
+
+
+def _eye(d: int) -> np.ndarray:
+    e = _EYES.get(d)
+    if e is None:
+        e = _EYES[d] = np.eye(d, dtype=np.complex128)
+    return e
 
 
 def classify(u: np.ndarray) -> str:
@@ -113,7 +123,7 @@ def lower_gate(gate, n: int, legacy_2q_order: bool = False) -> List[Op]:
     m = np.asarray(gate.matrix, dtype=np.complex128)
     if m.ndim != 2 or m.shape[0] != (1 << len(args)):
         raise ValueError(f"gate {tname}: matrix shape {m.shape} does not match {len(args)} qubits")
-    if np.array_equal(m, np.eye(m.shape[0])):
+    if m[0, 0] == 1 and np.array_equal(m, _eye(m.shape[0])):
         return []
     if _is_controlled(m, gate.controls, gate.targets):
         t = 1 << gate.targets
