@@ -63,13 +63,25 @@ def _batched_rotations(kind, thetas: np.ndarray, inverse: bool = False) -> Tuple
 
 class _Unit:
     """One op of the gradient circuit: a fixed gate, a parameterised gate, or a
-    group of commuting diagonal gates sharing one parameter (e.g. the Rzz gates
-    of a QAOA cost layer) merged into one diagonal on at most 4 qubits."""
+    group of gates sharing one parameter that commute: diagonal rotations (e.g.
+    the Rzz gates of a QAOA cost layer) merged into one diagonal on at most 4
+    qubits, or a pair of one-qubit rotations on different qubits (e.g. two Rx
+    of a QAOA mixer), whose unitary is the tensor product of theirs (`pair`)."""
 
     def __init__(self, entries: List[int], qubits: Tuple[int, ...], gen: Optional[np.ndarray] = None,
-                 fixed: Optional[np.ndarray] = None, index: int = -1, scale: float = 1.0):
+                 fixed: Optional[np.ndarray] = None, index: int = -1, scale: float = 1.0,
+                 pair: Optional[Tuple[np.ndarray, np.ndarray]] = None):
         self.entries, self.qubits, self.gen, self.fixed = entries, qubits, gen, fixed
-        self.index, self.scale = index, scale
+        self.index, self.scale, self.pair = index, scale, pair
+
+    def tables(self, thetas: np.ndarray, inverse: bool) -> Tuple[str, np.ndarray]:
+        """Per-instance tables of exp(-i theta G / 2) (see _batched_rotations)."""
+        if self.pair is None:
+            return _batched_rotations(self.gen, thetas, inverse)
+        _, a = _batched_rotations(self.pair[0], thetas, inverse)
+        _, b = _batched_rotations(self.pair[1], thetas, inverse)
+        u = np.einsum("bij,bkl->bikjl", a.reshape(-1, 2, 2), b.reshape(-1, 2, 2)).reshape(-1, 16)
+        return "mat", u
 
 
 def _diag_on(g: np.ndarray, qubits: Sequence[int], into: Sequence[int]) -> np.ndarray:
@@ -106,6 +118,25 @@ def gate_units(circuit: ParamCircuit, cluster: bool = True, max_qubits: int = 4)
             while (j < len(E) and E[j].kind != "fixed" and classify(GENERATORS[E[j].kind]) == "diag"
                    and E[j].index == e.index and E[j].scale == e.scale):
                 j += 1
+        if cluster and classify(g) != "diag" and len(e.qubits) == 1:
+            # one-qubit rotations with the same parameter on different qubits
+            # commute: pair them up as tensor products
+            seen = {e.qubits[0]}
+            while (j < len(E) and E[j].kind != "fixed" and len(E[j].qubits) == 1
+                   and classify(GENERATORS[E[j].kind]) != "diag" and E[j].index == e.index
+                   and E[j].scale == e.scale and E[j].qubits[0] not in seen):
+                seen.add(E[j].qubits[0])
+                j += 1
+            for t in range(i, j - 1, 2):
+                ga, gb = GENERATORS[E[t].kind], GENERATORS[E[t + 1].kind]
+                gen = np.kron(ga, np.eye(2)) + np.kron(np.eye(2), gb)
+                out.append(_Unit([t, t + 1], E[t].qubits + E[t + 1].qubits, gen=gen, index=e.index,
+                                 scale=e.scale, pair=(ga, gb)))
+            if (j - i) % 2:
+                t = j - 1
+                out.append(_Unit([t], E[t].qubits, gen=GENERATORS[E[t].kind], index=e.index, scale=e.scale))
+            i = j
+            continue
         if j - i == 1:
             out.append(_Unit([i], e.qubits, gen=g, index=e.index, scale=e.scale))
             i = j
@@ -179,7 +210,7 @@ class BatchedAdjoint:
                 k = classify(m)
                 out.append((i, Op("diag", tb, (), np.diag(m).copy()) if k == "diag" else Op(k, tb, (), m.copy())))
             else:
-                kind, tab = _batched_rotations(u.gen, u.scale * params[:, u.index], inverse)
+                kind, tab = u.tables(u.scale * params[:, u.index], inverse)
                 m0 = tab[0].copy() if kind == "diag" else tab[0].reshape(1 << len(tb), -1)
                 out.append((i, Op(kind, tb, (), m0, tag=("param", i), batch=tab)))
         return out

@@ -211,9 +211,10 @@ def test_pair_vector_backward_matches_shared_memory_path(cuda_ok, precision, tol
 
 def test_qaoa_cost_layer_units_match_the_gates():
     """Commuting Rzz gates that share a parameter are grouped into diagonal units
-    of at most 4 qubits; the units' product equals the gates' product."""
+    of at most 4 qubits, and Rx gates that share one into pairs; the units'
+    product equals the gates' product."""
     from quict_b200.differentiation import maxcut_observable, qaoa_circuit, random_regular_graph
-    from quict_b200.differentiation.adjoint import _batched_rotations, gate_units
+    from quict_b200.differentiation.adjoint import gate_units
     n, p = 8, 2
     edges = random_regular_graph(n, 3, np.random.default_rng(1))
     circ = qaoa_circuit(n, edges, p)
@@ -226,7 +227,7 @@ def test_qaoa_cost_layer_units_match_the_gates():
         if u.fixed is not None:
             mats.append((u.fixed, list(u.qubits)))
         else:
-            kind, tab = _batched_rotations(u.gen, np.array([u.scale * params[u.index]]))
+            kind, tab = u.tables(np.array([u.scale * params[u.index]]), False)
             m = np.diag(tab[0]) if kind == "diag" else tab[0].reshape(1 << len(u.qubits), -1)
             mats.append((m, list(u.qubits)))
     np.testing.assert_allclose(osv.run(mats, n), osv.run(circ.matrices(params), n), atol=1e-12)
