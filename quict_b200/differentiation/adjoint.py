@@ -175,14 +175,17 @@ class BatchedAdjoint:
         self.cdtype = torch.complex64 if precision == "single" else torch.complex128
         self.np_dtype = np.complex64 if precision == "single" else np.complex128
         k0, _ = default_tile(8 if precision == "single" else 16)
-        # the adjoint pass keeps two tiles (psi, lam) on chip
-        self.k = min(tile_bits or (k0 - 1), self.n)
+        # smallest register tile: 2^(R+5) amplitudes (R = 4 / 5 register bits)
+        min_k = 9 if precision == "double" else 10
+        # forward tiles; a small instance still gets a few tiles (CTAs), so
+        # that it does not run on one SM alone
+        self.k = min(tile_bits or max(min_k, min(k0 - 1, self.n - 3)), self.n)
         self.nlow = min(5, self.k)
-        # register-tile backward on the psi/lam pair vector: tile of k0 bits,
-        # one of them the pair bit; needs 2^(R+5) <= tile (R = 4 / 5)
-        self.pair_k = min(k0, self.n + 1)
-        self.pair_min_k = 9 if precision == "double" else 10
-        self.pair = pair and self.pair_k >= self.pair_min_k
+        # register-tile backward on the psi/lam pair vector: tile of up to k0
+        # bits, one of them the pair bit
+        self.pair_k = min(k0, max(min_k, self.n + 1 - 3))
+        self.pair_min_k = min_k
+        self.pair = pair and self.pair_min_k <= self.pair_k <= self.n + 1
         self.ws = Workspace(self.dev)
         self.launches = 0
         self.pauli = observable.masks()
@@ -301,7 +304,7 @@ class BatchedAdjoint:
         # with several instances the tile's non-pair bits must stay below the
         # instance bits, so the tile takes at most n of them
         pk = self.pair_k if bp == 1 else min(self.pair_k, self.n)
-        gp.pair = self.pair and pk >= self.pair_min_k
+        gp.pair = self.pair and self.pair_min_k <= pk <= nbits + 1
         if gp.pair:
             ops = [Op(o.kind, o.tbits, o.cbits, o.mat, tag=o.tag, batch=o.batch, slot=o.slot, extra=(nbits,))
                    if o.kind == "expect" else o for o in ops]
