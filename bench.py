@@ -478,7 +478,8 @@ def run_ours(args, ws, rank, local):
     n = args.qubits
     circuit = config1_circuit(n, N_GATES, SEED)
     sim = StateVectorSimulator("GPU", "double", gpu_device_id=local, sync=False,
-                               max_pass_cost=args.max_pass_cost, merge_bits=args.merge_bits)
+                               max_pass_cost=args.max_pass_cost, merge_bits=args.merge_bits,
+                               tile_bits=args.tile_bits)
     eng = sim.engine
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -613,6 +614,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
+    ap.add_argument("--tile-bits", type=int, default=None, help="fused tile width k (default: the tuning cache)")
     ap.add_argument("--merge-bits", type=int, default=None,
                     help="gate-merging block width (0 disables; default: the tuning cache)")
     ap.add_argument("--no-extra", action="store_true", help="skip the complex64 30q / 32q runs")
