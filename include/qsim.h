@@ -184,7 +184,7 @@ int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs_pass* pass
  * keeps each psi amplitude beside its lam partner, so EXPECT ops run on chip
  * between the gates.  partials: as for qs_adjoint_fused, ntiles = 2^(n - k).
  * Needs register tiles: k in [9, 12] (complex128) or [10, 13] (complex64),
- * nlow >= 5.  Replaces the same per-parameter re-runs as qs_adjoint_fused. */
+ * nlow >= 5; dense ops act on at most 2 bits.  Replaces the same per-parameter re-runs as qs_adjoint_fused. */
 int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* passes, int npasses,
                     const qs_op* ops, int64_t nops_total, const void* mats_dev, int64_t mats_count,
                     double* partials_dev, int64_t partials_count, void* stream);

@@ -577,7 +577,7 @@ __device__ __forceinline__ void r_expect_diag(const V (&x)[E], const V* __restri
     F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15) F(16) F(17) \
         F(18) F(19) F(20) F(21) F(22) F(23) F(24) F(25) F(26) F(27) F(28) F(29) F(30) F(31)
 
-template <typename V, int R, bool EXP>
+template <typename V, int R, bool EXP, bool BIG>
 __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* __restrict__ msm, uint32_t thr,
                                         uint64_t base, V* __restrict__ buf, const Addr<R>& ad,
                                         double2* __restrict__ ered) {
@@ -594,7 +594,7 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
         if constexpr ((MK) < (1 << R) && popc_c(MK) <= 2) {                          \
             if (pred) r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                 \
             else r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                     \
-        } else if constexpr ((MK) < (1 << R) && popc_c(MK) <= 4) {                   \
+        } else if constexpr (BIG && (MK) < (1 << R) && popc_c(MK) <= 4) {            \
             r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                           \
         }                                                                            \
         break;
@@ -738,8 +738,10 @@ __device__ __forceinline__ void tile_prefetch(V* __restrict__ dst, const V* __re
 }
 
 // EXP: adjoint pair pass (psi and lam halves in one vector, EXPECT ops write
-// per-tile partials to `partials`).
-template <typename V, int R, bool EXP>
+// per-tile partials to `partials`).  BIG: code paths for dense ops on 3 or 4
+// register bits; passes without such ops use the variant without them (less
+// code to fetch between the ops that do run).
+template <typename V, int R, bool EXP, bool BIG>
 __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const __grid_constant__ RegArgs p,
                                                       const V* __restrict__ mats, double* __restrict__ partials) {
     constexpr int E = 1 << R;
@@ -853,7 +855,7 @@ __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const
                 const KOp& op = sops[o];
                 if ((base & op.gctrl) != op.gctrl) continue;
                 if ((thr & op.tctrl) != op.tctrl) continue;
-                r_apply<V, R, EXP>(x, op, msm, thr, base, cur, ad, ered_w);
+                r_apply<V, R, EXP, BIG>(x, op, msm, thr, base, cur, ad, ered_w);
             }
         }
         {  // registers -> global in the last stage's layout (lanes on tile bits 0..4)
@@ -1292,10 +1294,10 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     return ndone;
 }
 
-template <typename V, int R, bool EXP>
-int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
+template <typename V, int R, bool EXP, bool BIG>
+int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
     static thread_local RegArgs args;
-    config_smem((const void*)k_fused_reg<V, R, EXP>);
+    config_smem((const void*)k_fused_reg<V, R, EXP, BIG>);
     std::vector<int> rem(ps.op_count);
     for (int i = 0; i < ps.op_count; ++i) rem[i] = i;
     while (!rem.empty()) {
@@ -1318,13 +1320,34 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
         // persistent grid: as many CTAs as fit on the SMs at once (smaller
         // tiles run several CTAs per SM, whose relayouts and arithmetic overlap)
         int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_reg<V, R, EXP>, threads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused_reg<V, R, EXP, BIG>, threads, smem);
         if (occ < 1) occ = 1;
         uint64_t cap = uint64_t(sm_count()) * uint64_t(occ);
-        k_fused_reg<V, R, EXP><<<unsigned(ntiles < cap ? ntiles : cap), threads, smem, st>>>(vec, args, mats, partials);
+        k_fused_reg<V, R, EXP, BIG><<<unsigned(ntiles < cap ? ntiles : cap), threads, smem, st>>>(vec, args, mats, partials);
         QS_CHECK_LAUNCH(EXP ? "qs_adjoint_pair" : "qs_apply_fused(reg)");
     }
     return QS_OK;
+}
+
+// Dense ops on 3 or 4 targets need the BIG kernel variant (forward passes
+// only: adjoint pair passes take dense ops on at most 2 bits).
+template <typename V, int R, bool EXP>
+int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
+    bool big = false;
+    for (int i = 0; i < ps.op_count; ++i) {
+        const qs_op& op = ops[ps.op_begin + i];
+        if (op.m >= 3 && op.kind != QS_OP_DIAG && !(op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG))) big = true;
+    }
+    if constexpr (EXP) {
+        if (big) {
+            set_error("qs_adjoint_pair: pass ops act densely on at most 2 bits");
+            return QS_EINVAL;
+        }
+        return launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st);
+    } else {
+        return big ? launch_reg_k<V, R, false, true>(vec, n, ps, ops, mats, partials, st)
+                   : launch_reg_k<V, R, false, false>(vec, n, ps, ops, mats, partials, st);
+    }
 }
 
 template <typename V>

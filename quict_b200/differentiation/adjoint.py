@@ -304,7 +304,10 @@ class BatchedAdjoint:
         # with several instances the tile's non-pair bits must stay below the
         # instance bits, so the tile takes at most n of them
         pk = self.pair_k if bp == 1 else min(self.pair_k, self.n)
-        gp.pair = self.pair and self.pair_min_k <= pk <= nbits + 1
+        # the pair kernel takes dense ops on at most 2 qubits
+        narrow = all(len(u.qubits) <= 2 or (u.fixed is None and classify(u.gen) == "diag")
+                     or (u.fixed is not None and classify(u.fixed) == "diag") for u in self._units)
+        gp.pair = self.pair and narrow and self.pair_min_k <= pk <= nbits + 1
         if gp.pair:
             ops = [Op(o.kind, o.tbits, o.cbits, o.mat, tag=o.tag, batch=o.batch, slot=o.slot, extra=(nbits,))
                    if o.kind == "expect" else o for o in ops]
