@@ -592,8 +592,12 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
 #define QS_CASE(MK)                                                                  \
     case MK:                                                                         \
         if constexpr ((MK) < (1 << R) && popc_c(MK) <= 2) {                          \
-            if (pred) r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                 \
-            else r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                     \
+            if constexpr (BIG || EXP) {                                              \
+                if (pred) r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);             \
+                else r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                 \
+            } else {                                                                 \
+                r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                      \
+            }                                                                        \
         } else if constexpr (BIG && (MK) < (1 << R) && popc_c(MK) <= 4) {            \
             r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);                           \
         }                                                                            \
@@ -739,8 +743,8 @@ __device__ __forceinline__ void tile_prefetch(V* __restrict__ dst, const V* __re
 
 // EXP: adjoint pair pass (psi and lam halves in one vector, EXPECT ops write
 // per-tile partials to `partials`).  BIG: code paths for dense ops on 3 or 4
-// register bits; passes without such ops use the variant without them (less
-// code to fetch between the ops that do run).
+// register bits and for dense ops with controls; passes without such ops use
+// the variant without them (less code to fetch between the ops that do run).
 template <typename V, int R, bool EXP, bool BIG>
 __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const __grid_constant__ RegArgs p,
                                                       const V* __restrict__ mats, double* __restrict__ partials) {
@@ -1329,14 +1333,21 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
     return QS_OK;
 }
 
-// Dense ops on 3 or 4 targets need the BIG kernel variant (forward passes
-// only: adjoint pair passes take dense ops on at most 2 bits).
+// Dense ops on 3 or 4 targets, and controlled dense ops, need the BIG kernel
+// variant (forward passes only: adjoint pair passes take dense ops on at most
+// 2 bits and keep the controlled paths).
 template <typename V, int R, bool EXP>
 int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
     bool big = false;
     for (int i = 0; i < ps.op_count; ++i) {
         const qs_op& op = ops[ps.op_begin + i];
-        if (op.m >= 3 && op.kind != QS_OP_DIAG && !(op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG))) big = true;
+        const bool diag = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+        if (op.m >= 3 && !diag) big = true;
+        // dense here: MAT, and the anti-diagonal / swap ops that are not plain
+        // exchanges (they run as dense matrices)
+        const bool dense = op.kind == QS_OP_MAT ||
+                           ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT));
+        if (dense && op.lctrl != 0 && !EXP) big = true;
     }
     if constexpr (EXP) {
         if (big) {
