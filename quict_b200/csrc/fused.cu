@@ -1083,18 +1083,20 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     }
     const int lowlanes = 5;  // tile bits 0..4 are the lanes of the load/store layout
     const uint32_t lanemask = (1u << lowlanes) - 1u;
-    auto make_stage = [&](uint32_t bits, KStage& S) {
+    // slot j <-> tile bit order[j] (the pair bit, when present, is slot 0)
+    auto make_stage = [&](uint32_t bits, KStage& S, const uint8_t* order) {
         int j = 0, i = 0;
-        if (pair_tile >= 0 && ((bits >> pair_tile) & 1)) S.R[j++] = uint8_t(pair_tile);
-        for (int b = 0; b < K; ++b) {
-            if ((bits >> b) & 1) {
-                if (b != pair_tile) S.R[j++] = uint8_t(b);
-            } else {
-                S.T[i++] = uint8_t(b);
-            }
-        }
+        for (; j < R; ++j) S.R[j] = order[j];
+        for (int b = 0; b < K; ++b)
+            if (!((bits >> b) & 1)) S.T[i++] = uint8_t(b);
         for (; j < 6; ++j) S.R[j] = 0;
         for (; i < 8; ++i) S.T[i] = 0;
+    };
+    auto plain_order = [&](uint32_t bits, uint8_t* order) {
+        int j = 0;
+        if (pair_tile >= 0 && ((bits >> pair_tile) & 1)) order[j++] = uint8_t(pair_tile);
+        for (int b = 0; b < K; ++b)
+            if (((bits >> b) & 1) && b != pair_tile) order[j++] = uint8_t(b);
     };
     // ---- dependency graph
     const int m = int(rem.size());
@@ -1176,10 +1178,66 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
         stage_bits.push_back(best);
         stage_ops.push_back(order);
     }
+    // ---- slot order per stage.  Register ops dispatch on (kind, slot mask),
+    // one code path each; ordering each stage's slots so that its ops reuse
+    // the paths earlier stages of this launch already run keeps the set of
+    // code paths in use (the instruction working set) small.
+    std::vector<std::array<uint8_t, 6>> orders(stage_bits.size());
+    std::vector<int> used_keys;
+    for (size_t st = 0; st < stage_bits.size(); ++st) {
+        uint8_t base_order[6] = {0};
+        plain_order(stage_bits[st], base_order);
+        // the ops' register targets (tile bits) and dispatch codes
+        std::vector<std::pair<int, uint32_t>> dense;
+        for (int pos : stage_ops[st]) {
+            const qs_op& op = ops[ps.op_begin + rem[pos]];
+            const bool dg = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+            if (dg) continue;
+            int code = op.kind;
+            if ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT)) code = QS_OP_MAT;
+            uint32_t tb = 0;
+            for (int j = 0; j < op.m; ++j) tb |= 1u << op.tgt[j];
+            dense.emplace_back(code, tb);
+        }
+        const int fixed0 = (pair_tile >= 0 && ((stage_bits[st] >> pair_tile) & 1)) ? 1 : 0;
+        uint8_t perm[6], best[6];
+        for (int j = 0; j < R; ++j) perm[j] = best[j] = base_order[j];
+        int best_new = 1 << 30, best_sum = 1 << 30;
+        std::sort(perm + fixed0, perm + R);
+        do {
+            int nnew = 0, sum = 0;
+            std::vector<int> keys;
+            for (const auto& d : dense) {
+                uint32_t mask = 0;
+                for (int j = 0; j < R; ++j)
+                    if ((d.second >> perm[j]) & 1) mask |= 1u << j;
+                const int key = d.first * 64 + int(mask);
+                sum += int(mask);
+                if (std::find(used_keys.begin(), used_keys.end(), key) == used_keys.end() &&
+                    std::find(keys.begin(), keys.end(), key) == keys.end()) {
+                    ++nnew;
+                    keys.push_back(key);
+                }
+            }
+            if (nnew < best_new || (nnew == best_new && sum < best_sum)) {
+                best_new = nnew;
+                best_sum = sum;
+                for (int j = 0; j < R; ++j) best[j] = perm[j];
+            }
+        } while (!dense.empty() && std::next_permutation(perm + fixed0, perm + R));
+        for (const auto& d : dense) {
+            uint32_t mask = 0;
+            for (int j = 0; j < R; ++j)
+                if ((d.second >> best[j]) & 1) mask |= 1u << j;
+            const int key = d.first * 64 + int(mask);
+            if (std::find(used_keys.begin(), used_keys.end(), key) == used_keys.end()) used_keys.push_back(key);
+        }
+        for (int j = 0; j < 6; ++j) orders[st][j] = j < R ? best[j] : 0;
+    }
     // ---- emit stages and translate each op into its stage's layout
     int ns = 0, nops = 0, moff = 0;
     for (size_t st = 0; st < stage_bits.size(); ++st) {
-        make_stage(stage_bits[st], a.st[ns]);
+        make_stage(stage_bits[st], a.st[ns], orders[st].data());
         a.st[ns].op_begin = uint16_t(nops);
         a.st[ns].op_count = 0;
         ++ns;
@@ -1270,7 +1328,9 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     if (last & lanemask) {
         uint32_t bits = 0;
         for (int b = K - 1, c = 0; b >= lowlanes && c < R; --b, ++c) bits |= 1u << b;
-        make_stage(bits, a.st[ns]);
+        uint8_t order[6] = {0};
+        plain_order(bits, order);
+        make_stage(bits, a.st[ns], order);
         a.st[ns].op_begin = uint16_t(nops);
         a.st[ns].op_count = 0;
         ++ns;
