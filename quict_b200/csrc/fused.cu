@@ -508,7 +508,7 @@ __device__ __forceinline__ void r_diag(V (&x)[E], const V* __restrict__ Dm, uint
 }
 
 // ---- diagonal, one code path for every slot mask: x[s] *= d[(h << ns) | kidx[s]]
-template <typename V, int E>
+template <typename V, int E, bool PRED>
 __device__ __forceinline__ void r_diag_any(V (&x)[E], const V* __restrict__ Dm, uint32_t scm, uint32_t h,
                                            const KOp& op) {
     const V* d = Dm + (h << op.ns);
@@ -520,9 +520,13 @@ __device__ __forceinline__ void r_diag_any(V (&x)[E], const V* __restrict__ Dm, 
         const uint32_t k = (kw[s >> 2] >> (8 * (s & 3))) & 0xffu;
         const V f = d[k];
         const V y = cmul(x[s], f);
-        const bool ok = (uint32_t(s) & scm) == scm;
-        x[s].x = ok ? y.x : x[s].x;
-        x[s].y = ok ? y.y : x[s].y;
+        if constexpr (PRED) {
+            const bool ok = (uint32_t(s) & scm) == scm;
+            x[s].x = ok ? y.x : x[s].x;
+            x[s].y = ok ? y.y : x[s].y;
+        } else {
+            x[s] = y;
+        }
     }
 }
 
@@ -667,7 +671,8 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
                 if (pred) r_diag<V, E, 0, true>(x, Mm, scm, h);
                 else r_diag<V, E, 0, false>(x, Mm, scm, h);
             } else {
-                r_diag_any<V, E>(x, Mm, scm, h, op);
+                if (pred) r_diag_any<V, E, true>(x, Mm, scm, h, op);
+                else r_diag_any<V, E, false>(x, Mm, scm, h, op);
             }
         }
     }
