@@ -571,7 +571,7 @@ def run_ours(args, ws, rank, local):
                      "unit": "TFLOP/s", "frac": fp64_achieved / fp64_peak, "peak_source": fp64_src,
                      "traffic": ncu_traffic(n), "algorithmic_flops_per_launch": flops / max(1, len(pass_list)),
                      "avg_launch_ms": avg_pass_ms,
-                     "note": "a fused pass applies ~30 merged ops per HBM round trip, so FP64 issue, not HBM, "
+                     "note": "a fused pass applies ~20 merged ops per HBM round trip, so FP64 issue, not HBM, "
                              "bounds it; roofline_hbm gives the HBM view"},
         "roofline_hbm": {"bound": "hbm", "kernel": "k_fused_reg", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(n),
