@@ -16,7 +16,8 @@ e2e     the same metric through the public API (StateVectorSimulator.run):
 roofline  the fused-pass kernel (k_fused_reg), bound fp64: algorithmic flops of
         its ops over its CUDA-event time, against cuBLAS DGEMM measured here;
         roofline_hbm: 2 * 2^n * 16 bytes per launch against MEASURED_PEAKS.json.
-single_gate_sweep, c64, adjoint, qaoa  extra sections.
+single_gate_sweep, c64, configs_0_2, adjoint, qaoa  extra sections: per-gate HBM
+        fractions, complex64 at 30/32 qubits, configs 0 and 2, gradients, QAOA batch.
 cpu_baseline  the numba port of the reference CPU kernels (oracle/ref_port.py)
         on this host's cores, on the first gates of the same circuit.
 """
