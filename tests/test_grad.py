@@ -3,7 +3,7 @@
 Pins: tests/golden/grad.npz holds energies and parameter-shift gradients
 computed from the REFERENCE StateVectorSimulator's amplitudes.  Tolerances:
 complex128 energies / gradients within 1e-10, complex64 within 1e-4 of the
-FP64 oracle (gradient error at most 1e-4 in complex64)."""
+FP64 oracle."""
 import numpy as np
 import pytest
 
