@@ -19,7 +19,8 @@ OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqsim.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "--split-compile", "0"]  # device code optimised in parallel (the fused kernels are large)
 
 
 def nvcc() -> str:

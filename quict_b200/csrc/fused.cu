@@ -596,7 +596,7 @@ __device__ __forceinline__ void r_apply(V (&x)[1 << R], const KOp& op, const V* 
 #define QS_CASE(MK)                                                                  \
     case MK:                                                                         \
         if constexpr ((MK) < (1 << R) && popc_c(MK) <= 2) {                          \
-            if constexpr (BIG || EXP) {                                              \
+            if constexpr (BIG) {                                                     \
                 if (pred) r_mat<V, E, R, MK, true>(x, Mm, scm, buf, ad);             \
                 else r_mat<V, E, R, MK, false>(x, Mm, scm, buf, ad);                 \
             } else {                                                                 \
@@ -1399,8 +1399,8 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
 }
 
 // Dense ops on 3 or 4 targets, and controlled dense ops, need the BIG kernel
-// variant (forward passes only: adjoint pair passes take dense ops on at most
-// 2 bits and keep the controlled paths).
+// variant (adjoint pair passes take dense ops on at most 2 bits; their BIG
+// variant only adds the controlled paths).
 template <typename V, int R, bool EXP>
 int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
     bool big = false;
@@ -1412,14 +1412,19 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
         // exchanges (they run as dense matrices)
         const bool dense = op.kind == QS_OP_MAT ||
                            ((op.kind == QS_OP_ANTI || op.kind == QS_OP_SWAP) && !(op.flags & QS_OPF_UNIT));
-        if (dense && op.lctrl != 0 && !EXP) big = true;
+        if (dense && op.lctrl != 0) big = true;
     }
     if constexpr (EXP) {
-        if (big) {
-            set_error("qs_adjoint_pair: pass ops act densely on at most 2 bits");
-            return QS_EINVAL;
+        for (int i = 0; i < ps.op_count; ++i) {
+            const qs_op& op = ops[ps.op_begin + i];
+            const bool diag = op.kind == QS_OP_DIAG || (op.kind == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+            if (op.m >= 3 && !diag) {
+                set_error("qs_adjoint_pair: pass ops act densely on at most 2 bits");
+                return QS_EINVAL;
+            }
         }
-        return launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st);
+        return big ? launch_reg_k<V, R, true, true>(vec, n, ps, ops, mats, partials, st)
+                   : launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st);
     } else {
         return big ? launch_reg_k<V, R, false, true>(vec, n, ps, ops, mats, partials, st)
                    : launch_reg_k<V, R, false, false>(vec, n, ps, ops, mats, partials, st);
