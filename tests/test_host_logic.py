@@ -238,3 +238,28 @@ def test_swap_relabelling_acts_like_the_swaps(seed):
         return v
 
     np.testing.assert_allclose(run(new), run(ops), atol=1e-12)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_merged_blocks_act_like_the_ops(seed):
+    """Gate merging (dense blocks on at most 2 tile bits, diagonal blocks on at
+    most 4 bits anywhere, also outside the tile) keeps the circuit's action."""
+    from quict_b200.core import Circuit
+    from quict_b200.simulation.fusion import _full_matrix, merge_ops
+    from quict_b200.simulation.lowering import lower_circuit
+    n = 7
+    c = Circuit(n)
+    c.random_append(90, seed=seed)
+    ops = lower_circuit(c.gates, n)
+    merged = merge_ops(ops, frozenset(range(4)), 2)   # bits 4..6 lie outside the tile
+    assert len(merged) < len(ops)
+    assert all(o.m <= 4 and (o.kind == "diag" or o.m <= 2 or o in ops) for o in merged)
+
+    def run(lst):
+        v = np.full(1 << n, 1 / np.sqrt(1 << n), dtype=np.complex128)
+        for op in lst:
+            bits, u = _full_matrix(op)
+            v = osv.apply_matrix(v, n, u, [n - 1 - b for b in bits])
+        return v
+
+    np.testing.assert_allclose(run(merged), run(ops), atol=1e-12)
