@@ -429,10 +429,14 @@ __device__ __forceinline__ void r_mat(V (&x)[E], const V* __restrict__ Mm, uint3
                     });
                     sfor<D>([&](auto rc) __attribute__((always_inline)) {
                         constexpr int r = decltype(rc)::value;
-                        V acc = cmul(PRELOAD ? mr[PRELOAD ? r * D : 0] : Mm[r * D], xi[0]);
+                        auto mat = [&](int e) -> V {
+                            if constexpr (PRELOAD) return mr[e];
+                            else return Mm[e];
+                        };
+                        V acc = cmul(mat(r * D), xi[0]);
 #pragma unroll
                         for (int c = 1; c < D; ++c)
-                            acc = cfma(PRELOAD ? mr[PRELOAD ? r * D + c : 0] : Mm[r * D + c], xi[c], acc);
+                            acc = cfma(mat(r * D + c), xi[c], acc);
                         x[s | pdep_c(r, MASK)] = acc;
                     });
                 }
@@ -503,7 +507,10 @@ __device__ __forceinline__ void r_diag(V (&x)[E], const V* __restrict__ Dm, uint
     sfor<E>([&](auto sc) __attribute__((always_inline)) {
         constexpr int s = decltype(sc)::value;
         constexpr int k = pext_c(s, SM);
-        if (!PRED || ctrl_ok(s, scm)) x[s] = cmul(x[s], PRELOAD ? dv[PRELOAD ? k : 0] : d[k]);
+        if (!PRED || ctrl_ok(s, scm)) {
+            if constexpr (PRELOAD) x[s] = cmul(x[s], dv[k]);
+            else x[s] = cmul(x[s], d[k]);
+        }
     });
 }
 
