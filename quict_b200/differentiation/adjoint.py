@@ -165,7 +165,8 @@ class BatchedAdjoint:
     """Energies and gradients of <psi(theta)|H|psi(theta)> for a batch of theta."""
 
     def __init__(self, circuit: ParamCircuit, observable: PauliSum, precision: str = "single",
-                 device_id: int = 0, tile_bits: Optional[int] = None, pair: bool = True):
+                 device_id: int = 0, tile_bits: Optional[int] = None, pair: bool = True,
+                 pair_tile_bits: Optional[int] = None):
         if observable.n != circuit.n:
             raise ValueError("observable and circuit act on different qubit counts")
         self.circuit = circuit
@@ -182,8 +183,11 @@ class BatchedAdjoint:
         self.k = min(tile_bits or max(min_k, min(k0 - 1, self.n - 3)), self.n)
         self.nlow = min(5, self.k)
         # register-tile backward on the psi/lam pair vector: tile of up to k0
-        # bits, one of them the pair bit
-        self.pair_k = min(k0, max(min_k, self.n + 1 - 3))
+        # bits, one of them the pair bit (two tile buffers of 2^k0 amplitudes
+        # fill 128 KB of shared memory: one CTA per SM)
+        if pair_tile_bits is not None and not min_k <= pair_tile_bits <= k0:
+            raise ValueError(f"pair_tile_bits must lie in [{min_k}, {k0}] for {precision} precision")
+        self.pair_k = pair_tile_bits or min(k0, max(min_k, self.n + 1 - 3))
         self.pair_min_k = min_k
         self.pair = pair and self.pair_min_k <= self.pair_k <= self.n + 1
         self.ws = Workspace(self.dev)

@@ -88,6 +88,7 @@ def main() -> None:
     """Run one workload on cuda:0 (for profiling a single kernel family):
 
         python -m quict_b200.workloads gradient --batch 256 [--precision single] [--repeat 2]
+            [--tile-bits K] [--pair-tile-bits K]
     """
     import argparse
 
@@ -98,10 +99,12 @@ def main() -> None:
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--tile-bits", type=int, default=None, help="forward register tile width k")
+    ap.add_argument("--pair-tile-bits", type=int, default=None, help="backward pair tile width k")
     a = ap.parse_args()
     from .differentiation import BatchedAdjoint
     circ, obs, params = config3_problem(16, 8, a.batch)
-    eng = BatchedAdjoint(circ, obs, a.precision)
+    eng = BatchedAdjoint(circ, obs, a.precision, tile_bits=a.tile_bits, pair_tile_bits=a.pair_tile_bits)
     gp = eng.plan_gradient(params)
     for _ in range(a.repeat):
         eng.launch(gp)

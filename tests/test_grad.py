@@ -209,6 +209,28 @@ def test_pair_vector_backward_matches_shared_memory_path(cuda_ok, precision, tol
     np.testing.assert_allclose(ga.cpu().numpy(), gb.cpu().numpy(), atol=tol * len(edges))
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol,widths", [("double", 1e-10, (9, 10, 11, 12)),
+                                                  ("single", 1e-4, (10, 11, 12, 13))])
+def test_pair_tile_widths_agree(cuda_ok, precision, tol, widths):
+    """Every pair tile width the register backward accepts gives the gradient
+    of the shared-memory backward; widths outside that range are refused."""
+    from quict_b200.differentiation import BatchedAdjoint
+    circ, obs = _hea(13, 2)  # batch of 2: the tile takes up to 13 non-pair bits
+    params = np.random.default_rng(6).uniform(0, 2 * np.pi, (2, circ.num_params))
+    e0, g0 = BatchedAdjoint(circ, obs, precision, pair=False).gradient(params)
+    for k in widths:
+        eng = BatchedAdjoint(circ, obs, precision, pair_tile_bits=k)
+        assert eng.plan_gradient(params).pair
+        e, g = eng.gradient(params)
+        np.testing.assert_allclose(e.cpu().numpy(), e0.cpu().numpy(), atol=tol)
+        # 13 qubits, 13 Ising terms: the two backward sweeps sum in different orders
+        np.testing.assert_allclose(g.cpu().numpy(), g0.cpu().numpy(), atol=4 * tol)
+    for k in (widths[0] - 1, widths[-1] + 1):
+        with pytest.raises(ValueError):
+            BatchedAdjoint(circ, obs, precision, pair_tile_bits=k)
+
+
 def test_qaoa_cost_layer_units_match_the_gates():
     """Commuting Rzz gates that share a parameter are grouped into diagonal units
     of at most 4 qubits, and Rx gates that share one into pairs; the units'
