@@ -169,15 +169,17 @@ class BatchedAdjoint:
                  pair_tile_bits: Optional[int] = None):
         if observable.n != circuit.n:
             raise ValueError("observable and circuit act on different qubit counts")
+        k0, _ = default_tile(8 if precision == "single" else 16)
+        # smallest register tile: 2^(R+5) amplitudes (R = 4 / 5 register bits)
+        min_k = 9 if precision == "double" else 10
+        if pair_tile_bits is not None and not min_k <= pair_tile_bits <= k0:
+            raise ValueError(f"pair_tile_bits must lie in [{min_k}, {k0}] for {precision} precision")
         self.circuit = circuit
         self.obs = observable
         self.n = circuit.n
         self.dev = require_cuda(device_id)
         self.cdtype = torch.complex64 if precision == "single" else torch.complex128
         self.np_dtype = np.complex64 if precision == "single" else np.complex128
-        k0, _ = default_tile(8 if precision == "single" else 16)
-        # smallest register tile: 2^(R+5) amplitudes (R = 4 / 5 register bits)
-        min_k = 9 if precision == "double" else 10
         # forward tiles; a small instance still gets a few tiles (CTAs), so
         # that it does not run on one SM alone
         self.k = min(tile_bits or max(min_k, min(k0 - 1, self.n - 3)), self.n)
@@ -185,8 +187,6 @@ class BatchedAdjoint:
         # register-tile backward on the psi/lam pair vector: tile of up to k0
         # bits, one of them the pair bit (two tile buffers of 2^k0 amplitudes
         # fill 128 KB of shared memory: one CTA per SM)
-        if pair_tile_bits is not None and not min_k <= pair_tile_bits <= k0:
-            raise ValueError(f"pair_tile_bits must lie in [{min_k}, {k0}] for {precision} precision")
         self.pair_k = pair_tile_bits or min(k0, max(min_k, self.n + 1 - 3))
         self.pair_min_k = min_k
         self.pair = pair and self.pair_min_k <= self.pair_k <= self.n + 1

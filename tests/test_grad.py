@@ -68,6 +68,17 @@ def test_pauli_masks_and_dense_matrix_agree():
     np.testing.assert_allclose(out, hs.matrix() @ v, atol=1e-14)
 
 
+def test_pair_tile_width_range_is_checked_before_the_device():
+    """pair_tile_bits outside [smallest register tile, 64 KiB tile] is refused
+    on the host, before any device is touched."""
+    from quict_b200.differentiation import BatchedAdjoint
+    circ, obs = _hea(4, 1)
+    for precision, bad in (("double", (8, 13)), ("single", (9, 14))):
+        for k in bad:
+            with pytest.raises(ValueError, match="pair_tile_bits"):
+                BatchedAdjoint(circ, obs, precision, pair_tile_bits=k)
+
+
 def test_random_regular_graph_is_regular():
     from quict_b200.differentiation import random_regular_graph
     for n in (10, 16, 24):
