@@ -69,13 +69,16 @@ class Op:
 
 
 def _is_controlled(m: np.ndarray, controls: int, targets: int) -> bool:
-    d = m.shape[0]
-    t = 1 << targets
+    """m = diag(I, U) with U on the last 2^targets rows / columns."""
     if controls == 0:
         return False
-    top = m[: d - t, : d - t]
-    return (np.array_equal(top, _eye(d - t))
-            and not np.any(m[: d - t, d - t:]) and not np.any(m[d - t:, : d - t]))
+    d = m.shape[0]
+    c = d - (1 << targets)
+    top = m[:c]
+    # the first c rows hold exactly c nonzeros (NaN counts as one), the c
+    # diagonal ones all equal to 1; nothing left of U in the last rows
+    return (np.count_nonzero(top) == c and bool(np.all(top.diagonal() == 1))
+            and not np.count_nonzero(m[c:, :c]))
 
 
 _EYES = {}
@@ -91,17 +94,18 @@ def _eye(d: int) -> np.ndarray:
 def classify(u: np.ndarray) -> str:
     """Structural kind of a target matrix (exact zero tests)."""
     d = u.shape[0]
-    off = u.copy()
-    np.fill_diagonal(off, 0)
-    if not np.any(off):
+    if d == 2:  # scalar tests: most gates are 1-qubit
+        if u[0, 1] == 0 and u[1, 0] == 0:
+            return "diag"
+        if u[0, 0] == 0 and u[1, 1] == 0:
+            return "antidiag"
+        return "mat"
+    # every nonzero (NaN counts as one) on the diagonal / on the swap pattern
+    nz = np.count_nonzero(u)
+    if nz == np.count_nonzero(u.diagonal()):
         return "diag"
-    if d == 2 and u[0, 0] == 0 and u[1, 1] == 0:
-        return "antidiag"
-    if d == 4:
-        mask = np.zeros((4, 4), dtype=bool)
-        mask[0, 0] = mask[1, 2] = mask[2, 1] = mask[3, 3] = True
-        if not np.any(u[~mask]):
-            return "swap"
+    if d == 4 and nz == sum(1 for x in (u[0, 0], u[1, 2], u[2, 1], u[3, 3]) if x != 0):
+        return "swap"
     return "mat"
 
 
@@ -141,7 +145,7 @@ def lower_gate(gate, n: int, legacy_2q_order: bool = False) -> List[Op]:
     tbits = tuple(n - 1 - q for q in tq)
     cbits = tuple(n - 1 - q for q in cq)
     if kind == "diag":
-        return [Op("diag", tbits, cbits, np.diag(u).copy())]
+        return [Op("diag", tbits, cbits, u.diagonal().copy())]
     return [Op(kind, tbits, cbits, u.copy())]
 
 
