@@ -103,6 +103,38 @@ def test_fusion_plan_preserves_semantics(seed, k, nlow, merge):
     np.testing.assert_allclose(got, ref, atol=1e-12)
 
 
+def _tiny_circuit(n, seed, size=30):
+    """Random circuit on n <= 3 qubits from every fixed-size gate type that fits."""
+    from quict_b200.core import Circuit, GATE_BY_NAME
+    from quict_b200.core.gate import GateType
+    types = [GateType[nm] for nm, g in GATE_BY_NAME.items()
+             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm")
+             and g.controls + g.targets <= n]
+    c = Circuit(n)
+    c.random_append(size, typelist=types, seed=seed)
+    return c
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+@pytest.mark.parametrize("merge", [0, 2])
+def test_fusion_plan_on_the_smallest_circuits(n, merge):
+    """1-3 qubit circuits: the planner clips the tile to the vector (k <= n,
+    nlow <= k), every op lands in a pass, and the passes act like the circuit."""
+    from quict_b200.simulation.fusion import Pass, iter_plan, relabel_swaps
+    from quict_b200.simulation.lowering import lower_circuit
+    for seed in range(4):
+        c = _tiny_circuit(n, seed)
+        ops = lower_circuit(c.gates, n)
+        steps = list(iter_plan(relabel_swaps(ops, n), n, 11, 5, merge_bits=merge))
+        flat = []
+        for s in steps:
+            assert isinstance(s, Pass)
+            assert len(set(range(min(5, n))) | set(s.hi)) == n and all(b < n for b in s.hi)
+            flat.extend(s.ops)
+        ref = osv.run(oracle_gates(c), n)
+        np.testing.assert_allclose(_apply_ops_oracle(osv.zero_state(n), n, flat), ref, atol=1e-12)
+
+
 def test_fusion_hoists_diagonal_and_controls():
     from quict_b200.core import Circuit, H, Rz, CZ, CX, Rzz
     from quict_b200.simulation.fusion import plan

@@ -215,3 +215,34 @@ def test_errors_are_raised_not_silently_ignored(cuda_ok):
     v = torch.zeros(8, dtype=torch.complex128, device="cuda")
     with pytest.raises(N.QsimError):
         N.call("qs_apply_1q", v.data_ptr(), 3, N.QS_C128, 5, 0, N.QS_K_DENSE, N.mat_ptr(np.eye(2))[1], None)
+
+
+@pytest.mark.parametrize("n", [1, 2])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_smallest_and_empty_circuits(cuda_ok, n, precision):
+    """1- and 2-qubit circuits from every fixed-size gate type that fits, fused
+    and gate by gate, against the oracle; an empty circuit leaves |0...0>;
+    sampling and P(0) on the smallest vectors."""
+    from quict_b200.core import Circuit, GATE_BY_NAME
+    from quict_b200.core.gate import GateType
+    types = [GateType[nm] for nm, g in GATE_BY_NAME.items()
+             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm")
+             and g.controls + g.targets <= n]
+    c = Circuit(n)
+    c.random_append(40, typelist=types, seed=n)
+    ref = osv.run(oracle_gates(c), n)
+    for fusion in (True, False):
+        s = sim(precision, fusion=fusion)
+        v = s.run(build_circuit([[g.type.name, g.cargs + g.targs, g.pargs] for g in c.gates], n, precision)).get()
+        np.testing.assert_allclose(v, ref, rtol=0, atol=TOL[precision])
+        u = np.random.default_rng(5).random(256)
+        s.sample(256, uniforms=u, mode="cdf")
+        got = s.last_sample_indices.cpu().numpy()
+        ties = osv.near_ties(ref, u, 1e-5)
+        assert np.all((got == osv.sample_cdf(ref, u)) | ties)
+        p0 = s.get_measured_prob(0)
+        assert abs(p0 - np.sum(np.abs(ref[0::2]) ** 2)) < 10 * TOL[precision]  # vector bit 0
+        e = sim(precision, fusion=fusion).run(Circuit(n)).get()
+        want = np.zeros(1 << n)
+        want[0] = 1
+        np.testing.assert_array_equal(e, want)
