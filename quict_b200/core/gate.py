@@ -249,10 +249,18 @@ class BasicGate:
 
     @property
     def matrix(self) -> Optional[np.ndarray]:
+        """A fresh copy in the gate's precision.  A parametrised matrix is
+        rebuilt only when the parameters change (kept with the gate)."""
         if self._static is not None:
             m = self._static
         elif self._matrix_fn is not None:
-            m = np.asarray(self._matrix_fn(self._pargs), dtype=np.complex128)
+            key = tuple(self._pargs)
+            cached = self.__dict__.get("_mcache")
+            if cached is not None and cached[0] == key:
+                m = cached[1]
+            else:
+                m = np.asarray(self._matrix_fn(self._pargs), dtype=np.complex128)
+                self._mcache = (key, m)
         else:
             return None
         return m.astype(self._precision)
@@ -401,6 +409,8 @@ class PermGate(BasicGate):
 
 def _make(t: GateType) -> BasicGate:
     c, tg, p, mt, fn = _SPEC[t]
+    if p == 0 and fn is not None:  # a fixed gate: its matrix is built once
+        return BasicGate(t, c, tg, p, mt, None, np.asarray(fn([]), dtype=np.complex128))
     return BasicGate(t, c, tg, p, mt, fn)
 
 

@@ -46,6 +46,25 @@ def test_lowering_reproduces_circuit():
     assert kinds >= {"mat", "diag", "antidiag", "swap"}
 
 
+def test_gate_matrix_follows_parameters_and_is_a_copy():
+    """Fixed matrices are built once and parametrised ones are kept per gate,
+    yet every access returns a fresh array that tracks the current pargs."""
+    from quict_b200.core import H, Rx
+    r = Rx(0.3)
+    a = r.matrix
+    a[...] = 0
+    np.testing.assert_allclose(r.matrix, [[np.cos(0.15), -1j * np.sin(0.15)], [-1j * np.sin(0.15), np.cos(0.15)]])
+    r.pargs = [1.1]
+    np.testing.assert_allclose(r.matrix[0, 0], np.cos(0.55))
+    r.pargs[0] = 2.0  # in-place change of the parameter list
+    np.testing.assert_allclose(r.matrix[0, 0], np.cos(1.0))
+    h = H.copy()
+    h.matrix[0, 0] = 5
+    np.testing.assert_allclose(H.matrix, np.array([[1, 1], [1, -1]]) / np.sqrt(2))
+    h.convert_precision()
+    assert h.matrix.dtype == np.complex64 and H.matrix.dtype == np.complex128
+
+
 def test_lowering_kinds_and_controls():
     from quict_b200.core import CX, CZ, Rz, Rzz, Swap, H, CCX, sqiSwap
     from quict_b200.simulation.lowering import lower_gate
