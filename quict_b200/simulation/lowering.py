@@ -114,25 +114,26 @@ def lower_gate(gate, n: int, legacy_2q_order: bool = False) -> List[Op]:
     tname = gate.type.name
     if tname in _SKIP:
         return []
-    args = list(gate.cargs) + list(gate.targs)
-    for a in args:
-        if not (0 <= a < n):
-            raise ValueError(f"gate {tname} argument {a} outside a {n}-qubit circuit")
+    cargs, targs = list(gate.cargs), list(gate.targs)
+    args = cargs + targs
+    if args and (min(args) < 0 or max(args) >= n):
+        bad = next(a for a in args if not 0 <= a < n)
+        raise ValueError(f"gate {tname} argument {bad} outside a {n}-qubit circuit")
     if tname == "measure":
         return [Op("measure", (n - 1 - gate.targ,), qubit=gate.targ)]
     if tname == "reset":
         return [Op("reset", (n - 1 - gate.targ,), qubit=gate.targ)]
     if tname == "perm":
         return [Op("perm", tuple(n - 1 - a for a in args), perm=tuple(int(p) for p in gate.pargs))]
-    m = np.asarray(gate.matrix, dtype=np.complex128)
+    m = np.array(gate.matrix, dtype=np.complex128)  # always our own copy
     if m.ndim != 2 or m.shape[0] != (1 << len(args)):
         raise ValueError(f"gate {tname}: matrix shape {m.shape} does not match {len(args)} qubits")
     if m[0, 0] == 1 and np.array_equal(m, _eye(m.shape[0])):
         return []
     if _is_controlled(m, gate.controls, gate.targets):
         t = 1 << gate.targets
-        u = m[-t:, -t:]
-        cq, tq = list(gate.cargs), list(gate.targs)
+        u = m[-t:, -t:].copy()
+        cq, tq = cargs, targs
     else:
         u = m
         cq, tq = [], args
@@ -142,11 +143,11 @@ def lower_gate(gate, n: int, legacy_2q_order: bool = False) -> List[Op]:
         # matrix with its argument order reversed (gate_function.py:153-220,
         # cpu_calculator.py:168-186); reproduce that on request.
         tq = tq[::-1]
-    tbits = tuple(n - 1 - q for q in tq)
-    cbits = tuple(n - 1 - q for q in cq)
+    tbits = tuple([n - 1 - q for q in tq])
+    cbits = tuple([n - 1 - q for q in cq])
     if kind == "diag":
         return [Op("diag", tbits, cbits, u.diagonal().copy())]
-    return [Op(kind, tbits, cbits, u.copy())]
+    return [Op(kind, tbits, cbits, u)]
 
 
 def lower_circuit(gates, n: int, legacy_2q_order: bool = False) -> List[Op]:
