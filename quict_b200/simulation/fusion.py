@@ -113,47 +113,44 @@ def iter_plan(ops: Sequence[Op], n: int, k: int, nlow: int, max_ops: int = N.QS_
     nlow = min(nlow, k)
     H = k - nlow
     low = frozenset(range(nlow))
-    pending = list(ops)
-    def fits(op: Op) -> bool:
-        return fusable(op) and len(op.xbits - low) <= H
 
+    # per-op facts the scan reads on every pass, computed once:
+    # (op, fits a tile, bits outside `low` it needs, conflict bits as a
+    #  writer, block-diagonal bits, all conflict bits, cost, table entries)
+    def facts(op: Op):
+        xb, zb = op.xbits, op.zbits
+        xc = xb - frozenset(op.extra)  # extra bits are tile requirements, not conflicts
+        xh = xb - low
+        return (op, fusable(op) and len(xh) <= H, xh, xc, zb, xc | zb, op_cost(op), op_entries(op))
+
+    pending = [facts(op) for op in ops]
     while pending:
         # leading ops that can never be tile-resident run on their own
-        if not fits(pending[0]):
-            yield Single(pending.pop(0))
+        if not pending[0][1]:
+            yield Single(pending.pop(0)[0])
             continue
         hi: set = set()
         chosen: List[Op] = []
-        deferred: List[Op] = []
+        deferred: list = []
         xblk: set = set()
         zblk: set = set()
         cost = 0.0
         entries = 0
-        stop = False
-        for idx, op in enumerate(pending):
-            if stop:
-                deferred.append(op)
-                continue
-            if not fits(op):
+        for idx, f in enumerate(pending):
+            op, fits, xh, xc, zb, allb, c, ent = f
+            if not fits:
                 # a barrier: nothing after it may be hoisted above it
-                deferred.append(op)
-                stop = True
-                continue
-            xb, zb = op.xbits, op.zbits
-            xc = xb - frozenset(op.extra)  # extra bits are tile requirements, not conflicts
-            allb = xc | zb
+                deferred.extend(pending[idx:])
+                break
             hoistable = not (allb & xblk) and not (xc & zblk)
-            need = xb - low - hi
-            c = op_cost(op)
-            ent = op_entries(op)
-            if (hoistable and len(hi) + len(need) <= H and len(chosen) < max_ops
+            if (hoistable and len(hi | xh) <= H and len(chosen) < max_ops
                     and entries + ent <= N.QS_MAX_PASS_MATS and (cost + c <= max_cost or not chosen)):
-                hi |= need
+                hi |= xh
                 chosen.append(op)
                 cost += c
                 entries += ent
             else:
-                deferred.append(op)
+                deferred.append(f)
                 xblk |= xc
                 zblk |= zb
         # fill unused tile bits with the lowest free bits (longer contiguous runs)
