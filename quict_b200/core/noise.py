@@ -62,6 +62,17 @@ class QuantumNoiseError:
     def kraus(self) -> List[np.ndarray]:
         return [np.sqrt(p) * m for m, p in self.operators]
 
+    def kraus_array(self) -> np.ndarray:
+        """The Kraus operators stacked, shape (count, 2^q, 2^q); built once and
+        rebuilt when `operators` is replaced.  Read-only: it is shared."""
+        ops = self.operators
+        c = self.__dict__.get("_kraus_cache")
+        if c is None or c[0] is not ops or c[1] != len(ops):
+            arr = np.sqrt(np.array([p for _, p in ops], dtype=np.float64))[:, None, None] * np.array([m for m, _ in ops])
+            arr.setflags(write=False)
+            c = self._kraus_cache = (ops, len(ops), arr)
+        return c[2]
+
     @property
     def kraus_ct(self) -> List[np.ndarray]:
         return [np.conj(k.T) for k in self.kraus]
@@ -94,10 +105,14 @@ class QuantumNoiseError:
         return QuantumNoiseError([(np.kron(a, b), pa * pb) for a, pa in self.operators for b, pb in other.operators])
 
     def apply_to_gate(self, matrix: np.ndarray) -> List[np.ndarray]:
+        return list(self.apply_to_gate_array(matrix))
+
+    def apply_to_gate_array(self, matrix: np.ndarray) -> np.ndarray:
+        """K_i @ matrix for every Kraus operator, stacked (one batched product)."""
         m = np.asarray(matrix, dtype=np.complex128)
         if m.shape != (1 << self._qubits, 1 << self._qubits):
             raise ValueError("gate matrix size does not match the noise's qubit number")
-        return [k @ m for k in self.kraus]
+        return np.matmul(self.kraus_array(), m)
 
     def prob_mapping_operator(self, prob: float) -> np.ndarray:
         for m, p in self.operators:
@@ -193,7 +208,17 @@ class NoiseGate:
     """Kraus operators standing in for a gate (QuICT/core/operator/noise_gate.py:6-35)."""
 
     def __init__(self, noise_matrix: List[np.ndarray], args_num: int):
-        self.noise_matrix = [np.asarray(k) for k in noise_matrix]
+        # a stacked (count, d, d) array is also kept whole for the simulators;
+        # noise_matrix then holds read-only views of it
+        if isinstance(noise_matrix, np.ndarray) and noise_matrix.ndim == 3:
+            stack = np.array(noise_matrix)  # own copy: the caller's array stays writable
+            stack.setflags(write=False)
+            self._stack = stack
+            self.noise_matrix = list(stack)
+            self._views = tuple(self.noise_matrix)
+        else:
+            self._stack = None
+            self.noise_matrix = [np.asarray(k) for k in noise_matrix]
         self.targets = args_num
         self.targs: List[int] = []
         self.cargs: List[int] = []
@@ -202,6 +227,16 @@ class NoiseGate:
     def __and__(self, targets):
         self.targs = [targets] if isinstance(targets, int) else list(targets)
         return self
+
+    def kraus_stack(self) -> Optional[np.ndarray]:
+        """The stacked Kraus operators, or None when there is no stack or
+        `noise_matrix` no longer holds exactly its views."""
+        if self._stack is None:
+            return None
+        nm = self.noise_matrix
+        if len(nm) != len(self._views) or any(a is not b for a, b in zip(nm, self._views)):
+            return None
+        return self._stack
 
     def __or__(self, circuit):
         circuit.append(self)
@@ -247,7 +282,7 @@ class NoiseModel:
                 for noise, qubits in self._error_by_gate[g.type.name]:
                     if qubits == -1 or set(args) <= set(qubits):
                         if accumulated_mode or noise.type == NoiseChannel.damping:
-                            ng = NoiseGate(noise.apply_to_gate(g.matrix), len(args))
+                            ng = NoiseGate(noise.apply_to_gate_array(g.matrix), len(args))
                             ng.targs = list(args)
                             out.gates.append(ng)
                             keep = False

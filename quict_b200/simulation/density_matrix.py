@@ -33,12 +33,19 @@ def _is_noise_gate(g) -> bool:
     return hasattr(g, "noise_matrix")
 
 
-def superop(kraus: List[np.ndarray]) -> np.ndarray:
-    """S = sum_i K_i (x) conj(K_i): (S vec(rho))[(r, c)] = sum K rho K^dagger."""
-    k = np.asarray([np.asarray(m, dtype=np.complex128) for m in kraus])
-    d = k.shape[1]
-    # S[(a, c), (b, d)] = sum_i K_i[a, b] conj(K_i[c, d]), all Kraus operators at once
-    return np.einsum("kab,kcd->acbd", k, k.conj()).reshape(d * d, d * d)
+def superop(kraus) -> np.ndarray:
+    """S = sum_i K_i (x) conj(K_i): (S vec(rho))[(r, c)] = sum K rho K^dagger.
+    `kraus` is a list of matrices or a stacked (count, d, d) array."""
+    if isinstance(kraus, np.ndarray) and kraus.ndim == 3:
+        k = kraus.astype(np.complex128, copy=False)
+    else:
+        k = np.asarray([np.asarray(m, dtype=np.complex128) for m in kraus])
+    cnt, d = k.shape[0], k.shape[1]
+    # S[(a, c), (b, d)] = sum_i K_i[a, b] conj(K_i[c, d]): one (d^2 x count) x
+    # (count x d^2) product over all Kraus operators, then a reordering
+    a = k.reshape(cnt, d * d)
+    m = a.T @ a.conj()  # m[(a, b), (c, d)]
+    return np.ascontiguousarray(m.reshape(d, d, d, d).transpose(0, 2, 1, 3)).reshape(d * d, d * d)
 
 
 def lower_dm(g, n: int, legacy_2q_order: bool = False) -> List[Op]:
@@ -47,7 +54,8 @@ def lower_dm(g, n: int, legacy_2q_order: bool = False) -> List[Op]:
         args = list(g.targs)
         rows = tuple(2 * n - 1 - q for q in args)
         cols = tuple(n - 1 - q for q in args)
-        s = superop(g.noise_matrix)
+        stack = g.kraus_stack() if hasattr(g, "kraus_stack") else None
+        s = superop(stack if stack is not None else g.noise_matrix)
         kind = classify(s)
         if kind == "diag":
             return [Op("diag", rows + cols, (), np.diag(s).copy())]

@@ -62,6 +62,38 @@ def test_transpile_attaches_one_noise_gate_per_matched_gate():
     assert len(t.gates[0].noise_matrix) == 8 and len(t.gates[1].noise_matrix) == 64
 
 
+def test_stacked_kraus_operators_and_superoperator():
+    """The batched Kraus path (stacked operators, one product per gate, one
+    GEMM per superoperator) equals the per-operator definitions; a noise gate
+    whose matrices were replaced falls back to them."""
+    from quict_b200.core import DampingError, DepolarizingError, H, CX
+    from quict_b200.core.noise import NoiseGate
+    from quict_b200.simulation.density_matrix import superop
+    amp = DampingError(amplitude_prob=0.05, phase_prob=0.02)
+    err = amp.tensor(amp).compose(DepolarizingError(0.03, 2))
+    g = CX.matrix
+    want = [k @ g for k in err.kraus]
+    got = err.apply_to_gate(g)
+    assert len(got) == len(want) == 144  # (3 damping operators)^2 x 16 Pauli products
+    np.testing.assert_allclose(np.array(got), np.array(want), rtol=0, atol=1e-15)
+    ng = NoiseGate(err.apply_to_gate_array(g), 2)
+    k = np.array(want)
+    ref = np.einsum("kab,kcd->acbd", k, k.conj()).reshape(16, 16)
+    np.testing.assert_allclose(superop(ng.kraus_stack()), ref, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(superop(ng.noise_matrix), ref, rtol=0, atol=1e-15)
+    with pytest.raises(ValueError):
+        ng.noise_matrix[0][0, 0] = 1  # views of the shared stack are read-only
+    ng.noise_matrix[0] = np.eye(4)
+    assert ng.kraus_stack() is None
+    # replacing an error's operators rebuilds its stack
+    e1 = amp.compose(DepolarizingError(0.01, 1))
+    s1 = e1.kraus_array()
+    e1.operators = e1.operators[:2]
+    assert e1.kraus_array().shape[0] == 2 and s1.shape[0] > 2
+    np.testing.assert_allclose(e1.apply_to_gate_array(H.matrix), np.array([k @ H.matrix for k in e1.kraus]),
+                               rtol=0, atol=1e-15)
+
+
 def test_readout_error_is_a_confusion_row_draw():
     from quict_b200.core import ReadoutError, Circuit
     err = ReadoutError([[0.0, 1.0], [1.0, 0.0]])  # always flips
