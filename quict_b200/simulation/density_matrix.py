@@ -211,4 +211,4 @@ class DensityMatrixSimulator:
                 nm.apply_readout_error(qs)
                 counts[int(qs)] += 1
             return counts.tolist()
-        return self._engine.histogram(idx, 1 << n).cpu().numpy().tolist()
+        return self._engine.counts_list(idx, 1 << n)

@@ -227,3 +227,18 @@ class Engine:
         N.call("qs_histogram", C.c_void_p(idx.data_ptr()), idx.numel(), C.c_void_p(counts.data_ptr()), ncounts,
                self.stream)
         return counts
+
+    def counts_list(self, idx: torch.Tensor, ncounts: int) -> list:
+        """Histogram of sample indices as a Python list of length `ncounts`.
+        With few shots per bin only the nonzero bins cross to the host, and the
+        list is a zero list with those entries set (a full ``tolist`` of 2^20
+        counts costs several ms)."""
+        counts = self.histogram(idx, ncounts)
+        if ncounts <= 4 * idx.numel():
+            return counts.cpu().numpy().tolist()
+        nz = torch.nonzero(counts).flatten()
+        where, vals = nz.cpu().tolist(), counts[nz].cpu().tolist()
+        out = [0] * ncounts
+        for i, c in zip(where, vals):
+            out[i] = c
+        return out

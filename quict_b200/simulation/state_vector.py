@@ -277,8 +277,7 @@ class StateVectorSimulator:
         self.last_sample_indices = idx
         if not return_counts:
             return idx
-        counts = self._engine.histogram(idx, 1 << n)
-        return counts.cpu().numpy().tolist()
+        return self._engine.counts_list(idx, 1 << n)
 
 
 def _is_trigger(g) -> bool:

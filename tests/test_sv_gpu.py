@@ -246,3 +246,26 @@ def test_smallest_and_empty_circuits(cuda_ok, n, precision):
         want = np.zeros(1 << n)
         want[0] = 1
         np.testing.assert_array_equal(e, want)
+
+
+def test_sample_counts_list_sparse_and_dense(cuda_ok):
+    """Counts come back as a list of length 2^n (as the reference returns), the
+    same whether few bins are hit (only nonzero bins are copied back) or many."""
+    from quict_b200.core import Circuit
+    from quict_b200.simulation import DensityMatrixSimulator
+    c = Circuit(12)
+    c.random_append(60, seed=12)
+    s = sim()
+    s.run(c)
+    for shots in (300, 20000):  # 4096 bins: fewer and more than 4 shots per bin
+        counts = s.sample(shots, seed=shots)
+        idx = s.last_sample_indices.cpu().numpy()
+        assert isinstance(counts, list) and len(counts) == 4096 and sum(counts) == shots
+        assert counts == np.bincount(idx, minlength=4096).tolist()
+    c6 = Circuit(6)
+    c6.random_append(30, seed=6)
+    dm = DensityMatrixSimulator("GPU")
+    dm.run(c6)
+    counts = dm.sample(10, seed=1)
+    idx = dm.last_sample_indices.cpu().numpy()
+    assert isinstance(counts, list) and counts == np.bincount(idx, minlength=64).tolist()
