@@ -30,6 +30,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -65,8 +66,10 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.csv"
+        # raw samples go to $QS_CLOCKS_DIR (default: the temp directory); the
+        # JSON line carries their summary
+        d = os.environ.get("QS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
