@@ -36,7 +36,8 @@ _SWAP = np.eye(4, dtype=np.complex128)[[0, 2, 1, 3]]
 
 
 class ShardedStateVector:
-    """An n-qubit state vector over all ranks of `group` (a power of two).
+    """An n-qubit state vector over all ranks of `group` (a power of two);
+    without an initialised process group, one unsplit vector on this device.
 
     ``backend`` runs the local work on one shard: ``apply_ops(vec, n, ops)``,
     ``prob0(vec, n, bit)`` and ``norm2(vec, n)`` -- by default the CUDA engine
@@ -47,8 +48,10 @@ class ShardedStateVector:
     def __init__(self, n: int, precision: str = "double", group=None, device: Optional[torch.device] = None,
                  backend=None, chunk_bytes: int = 1 << 28):
         self.group = group
-        self.world = dist.get_world_size(group)
-        self.rank = dist.get_rank(group)
+        # without a process group the vector is one unsplit shard on this device
+        self.solo = group is None and not dist.is_initialized()
+        self.world = 1 if self.solo else dist.get_world_size(group)
+        self.rank = 0 if self.solo else dist.get_rank(group)
         if self.world & (self.world - 1):
             raise ValueError(f"the number of ranks must be a power of two, got {self.world}")
         self.g = self.world.bit_length() - 1
@@ -59,7 +62,7 @@ class ShardedStateVector:
         self.dtype = torch.complex128 if precision == "double" else torch.complex64
         if backend is None:
             from .engine import Engine, require_cuda
-            device = device or require_cuda(torch.cuda.current_device())
+            device = device or require_cuda(torch.cuda.current_device() if torch.cuda.is_available() else 0)
             backend = Engine(device)
         self.backend = backend
         self.device = device if device is not None else torch.device("cpu")
@@ -212,6 +215,8 @@ class ShardedStateVector:
         self._flush(pending)
 
     def _sum_over_ranks(self, x: float) -> float:
+        if self.solo:
+            return float(x)
         dev = self.device if dist.get_backend(self.group) == "nccl" else torch.device("cpu")
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, group=self.group)
@@ -233,6 +238,8 @@ class ShardedStateVector:
         """The full vector on rank `dst` (after ``canonical``), None elsewhere;
         for vectors that fit one host."""
         self.canonical()
+        if self.solo:
+            return self.local.detach().cpu().numpy()
         src = torch.view_as_real(self.local.detach())
         if dist.get_backend(self.group) != "nccl":
             src = src.cpu()

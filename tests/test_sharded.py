@@ -145,3 +145,32 @@ def test_placement_of_rank_bit_controls_and_diagonals():
     assert op.tbits == (0,) and list(op.mat) == [1j, 1j]
     sv.rank = 0
     assert sv._place(Op("diag", (3,), (), np.array([1, 1j])), []) is None
+
+
+def test_solo_vector_on_cpu_stand_in():
+    """Without a process group: one unsplit vector, same API."""
+    from conftest import oracle_gates
+    from oracle import sv as osv
+    from quict_b200.simulation.sharded import ShardedStateVector
+    c = _circuit(6, 9, 50)
+    sv = ShardedStateVector(6, backend=_NumpyShard()).run(c)
+    ref = osv.run(oracle_gates(c), 6)
+    np.testing.assert_allclose(sv.gather(), ref, rtol=0, atol=1e-12)
+    assert sv.exchanges == 0 and abs(sv.norm2() - 1) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("double", 1e-12), ("single", 1e-5)])
+def test_solo_vector_on_the_gpu_engine(cuda_ok, precision, tol):
+    """The default backend (the CUDA engine) drives the shard: one process, no
+    process group, a 12-qubit circuit with 1-3 qubit gates."""
+    from conftest import oracle_gates
+    from oracle import sv as osv
+    from quict_b200.simulation.sharded import ShardedStateVector
+    c = _circuit(12, 4, 120)
+    sv = ShardedStateVector(12, precision).run(c)
+    ref = osv.run(oracle_gates(c), 12)
+    np.testing.assert_allclose(sv.gather(), ref, rtol=0, atol=tol)
+    assert abs(sv.norm2() - 1) < 10 * tol
+    want = float(np.sum(np.abs(ref[: 1 << 11]) ** 2))  # qubit 0 = vector bit 11
+    assert abs(sv.prob0(0) - want) < 10 * tol
