@@ -24,6 +24,7 @@ kernel waits on another rank: the exchange is a library send/recv pair.
 """
 from __future__ import annotations
 
+import bisect
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -116,15 +117,29 @@ class ShardedStateVector:
         self.exchanges += 1
 
     # ---- placing one op -----------------------------------------------------------------
-    def _free_local(self, busy: set) -> int:
-        """Highest local physical bit not in `busy` (high bits keep the low,
-        warp-contiguous bits out of the exchanges)."""
+    def _free_local(self, busy: set, at: int = -1) -> int:
+        """The local physical bit to trade for a rank bit: not in `busy`, and
+        holding the logical bit whose next dense use (after op `at` of the
+        current ``apply_ops``) is farthest away, so it can stay on a rank bit
+        longest (Belady's rule); ties go to the highest bit, which keeps the
+        low, warp-contiguous bits out of the exchanges."""
+        uses = getattr(self, "_uses", None)
+        best, best_next = -1, -1
         for p in range(self.nl - 1, -1, -1):
-            if p not in busy:
+            if p in busy:
+                continue
+            if uses is None:
                 return p
-        raise ValueError("no free local bit for an exchange: too few local bits for this op")
+            u = uses[self.where.index(p)]
+            k = bisect.bisect_right(u, at)
+            nxt = u[k] if k < len(u) else 1 << 62
+            if nxt > best_next:
+                best, best_next = p, nxt
+        if best < 0:
+            raise ValueError("no free local bit for an exchange: too few local bits for this op")
+        return best
 
-    def _place(self, op: Op, pending: List[Op]) -> Optional[Op]:
+    def _place(self, op: Op, pending: List[Op], at: int = -1) -> Optional[Op]:
         """The op in physical local bits for this rank, or None where it does
         nothing here.  Exchanges that the op needs flush `pending` first."""
         if op.kind not in ("mat", "diag", "antidiag", "swap"):
@@ -135,7 +150,7 @@ class ShardedStateVector:
                 p = self.where[b]
                 if p >= self.nl:
                     busy = {self.where[x] for x in op.tbits + op.cbits}
-                    self.exchange(p, self._free_local(busy))
+                    self.exchange(p, self._free_local(busy, at))
         tp = [self.where[b] for b in op.tbits]
         cp = [self.where[b] for b in op.cbits]
         if any(p >= self.nl and not self._rank_bit(p) for p in cp):
@@ -176,12 +191,23 @@ class ShardedStateVector:
     # ---- public surface -------------------------------------------------------------------
     def apply_ops(self, ops: Sequence[Op]):
         """Apply lowered ops (logical vector bits) in order."""
+        ops = list(ops)
+        # positions where each logical bit is a dense (non-diagonal) target:
+        # the lookahead of the exchange choice
+        self._uses = [[] for _ in range(self.n)]
+        for i, op in enumerate(ops):
+            if op.kind != "diag":
+                for b in op.tbits:
+                    self._uses[b].append(i)
         pending: List[Op] = []
-        for op in ops:
-            placed = self._place(op, pending)
-            if placed is not None:
-                pending.append(placed)
-        self._flush(pending)
+        try:
+            for i, op in enumerate(ops):
+                placed = self._place(op, pending, i)
+                if placed is not None:
+                    pending.append(placed)
+            self._flush(pending)
+        finally:
+            self._uses = None
 
     def run(self, circuit) -> "ShardedStateVector":
         """Apply a circuit's unitary gates from the current state (|0...0> at

@@ -174,3 +174,37 @@ def test_solo_vector_on_the_gpu_engine(cuda_ok, precision, tol):
     assert abs(sv.norm2() - 1) < 10 * tol
     want = float(np.sum(np.abs(ref[: 1 << 11]) ** 2))  # qubit 0 = vector bit 11
     assert abs(sv.prob0(0) - want) < 10 * tol
+
+
+def test_exchange_choice_looks_ahead():
+    """Dry run of the placement (bit map only): a rank bit is traded for the
+    local bit whose next dense use is farthest away, so a config-1 style
+    circuit (targets mostly in the low and high bits) needs about one
+    exchange per rank bit instead of one per dense gate on a rank bit."""
+    from quict_b200.simulation.lowering import lower_circuit
+    from quict_b200.simulation.sharded import ShardedStateVector
+    from quict_b200.workloads import config1_circuit
+
+    class Dry(ShardedStateVector):
+        def __init__(self, n, world):
+            self.n, self.world, self.rank = n, world, 0
+            self.g = world.bit_length() - 1
+            self.nl = n - self.g
+            self.where = list(range(n))
+            self.exchanges = 0
+
+        def exchange(self, gbit, lbit):
+            self._swap_roles(gbit, lbit)
+            self.exchanges += 1
+
+        def _flush(self, pending):
+            pending.clear()
+
+    n = 24
+    ops = lower_circuit(config1_circuit(n, 600, seed=3).gates, n)
+    for world in (2, 8):
+        d = Dry(n, world)
+        d.apply_ops(ops)
+        hits = sum(1 for o in ops if o.kind != "diag" and any(b >= d.nl for b in o.tbits))
+        assert 0 < d.exchanges <= 2 * d.g < hits
+        assert sorted(d.where) == list(range(n))
