@@ -13,6 +13,7 @@ A lowered op is placed against the current logical -> physical bit map:
   them where the rank's bit is 1 and is skipped where it is 0;
 - a diagonal op with global targets keeps only the entries that match the
   rank's bits (a diagonal on the remaining local targets, or one phase);
+- a plain SWAP gate only relabels (the two logical bits trade physical bits);
 - any other op with a global target first swaps that global bit with a free
   local bit: the two partner ranks (rank ^ 2^j) exchange the half of their
   shard whose local bit differs from their rank bit, point to point (NCCL
@@ -31,6 +32,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
+from .fusion import _unit_swap
 from .lowering import Op, lower_gate
 
 _SWAP = np.eye(4, dtype=np.complex128)[[0, 2, 1, 3]]
@@ -144,6 +146,11 @@ class ShardedStateVector:
         nothing here.  Exchanges that the op needs flush `pending` first."""
         if op.kind not in ("mat", "diag", "antidiag", "swap"):
             raise ValueError(f"sharded state vectors apply unitary ops only, not {op.kind}")
+        if _unit_swap(op):
+            # a plain SWAP only relabels: the two logical bits trade physical bits
+            a, b = op.tbits
+            self.where[a], self.where[b] = self.where[b], self.where[a]
+            return None
         if op.kind != "diag" and any(self.where[b] >= self.nl for b in op.tbits):
             self._flush(pending)
             for b in op.tbits:
@@ -196,7 +203,7 @@ class ShardedStateVector:
         # the lookahead of the exchange choice
         self._uses = [[] for _ in range(self.n)]
         for i, op in enumerate(ops):
-            if op.kind != "diag":
+            if op.kind != "diag" and not _unit_swap(op):
                 for b in op.tbits:
                     self._uses[b].append(i)
         pending: List[Op] = []
