@@ -32,6 +32,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
+from .. import _native as N
 from .fusion import _unit_swap
 from .lowering import Op, lower_gate
 
@@ -266,6 +267,49 @@ class ShardedStateVector:
         else:
             mine = 0.0 if self._rank_bit(p) else self.backend.norm2(self.local, self.nl)
         return self._sum_over_ranks(mine)
+
+    def _reduce_dev(self):
+        return self.device if (not self.solo and dist.get_backend(self.group) == "nccl") else torch.device("cpu")
+
+    def sample(self, shots: int, uniforms=None, seed: Optional[int] = None) -> np.ndarray:
+        """Basis indices of `shots` samples, one uniform per shot, on every
+        rank: the smallest global index i with u <= CDF[i] (FP64), the rule of
+        ``StateVectorSimulator.sample(mode="cdf")``.  The shot's rank comes
+        from the cumulative shard masses; that rank then finds the index in its
+        own shard for u minus the mass of the ranks before it.  `uniforms`, if
+        given, must be the same on every rank; otherwise rank 0 draws them
+        (numpy ``default_rng(seed)``) and broadcasts them."""
+        self.canonical()
+        dev = self._reduce_dev()
+        if uniforms is None:
+            u = torch.as_tensor(np.random.default_rng(seed).random(shots) if self.rank == 0 else np.zeros(shots),
+                                dtype=torch.float64)
+            if not self.solo:
+                u = u.to(dev)
+                dist.broadcast(u, 0 if self.group is None else dist.get_global_rank(self.group, 0), group=self.group)
+            u = u.cpu().numpy()
+        else:
+            u = np.asarray(uniforms, dtype=np.float64).ravel()[:shots]
+        mass = torch.tensor([self.backend.norm2(self.local, self.nl)], dtype=torch.float64, device=dev)
+        if not self.solo:
+            parts = [torch.empty_like(mass) for _ in range(self.world)]
+            dist.all_gather(parts, mass, group=self.group)
+            mass = torch.cat(parts)
+        cdf = np.cumsum(mass.cpu().numpy())
+        owner = np.minimum(np.searchsorted(cdf, u, side="left"), self.world - 1)
+        mine = np.flatnonzero(owner == self.rank)
+        out = np.zeros(shots, dtype=np.int64)
+        if mine.size:
+            before = cdf[self.rank - 1] if self.rank > 0 else 0.0
+            ul = torch.as_tensor(u[mine] - before, dtype=torch.float64)
+            idx = self.backend.sample_indices(self.local, self.nl, ul, N.QS_SAMPLE_CDF)
+            out[mine] = (np.asarray(idx.cpu().numpy() if hasattr(idx, "cpu") else idx, dtype=np.int64)
+                         + (self.rank << self.nl))
+        if self.solo:
+            return out
+        t = torch.as_tensor(out).to(dev)
+        dist.all_reduce(t, group=self.group)  # every shot is filled by exactly one rank
+        return t.cpu().numpy()
 
     def gather(self, dst: int = 0) -> Optional[np.ndarray]:
         """The full vector on rank `dst` (after ``canonical``), None elsewhere;

@@ -49,6 +49,11 @@ class _NumpyShard:
         idx = np.arange(v.size)
         return float(np.sum(np.abs(v[(idx >> bit) & 1 == 0]) ** 2))
 
+    def sample_indices(self, vec, n, uniforms, mode):
+        # smallest i with u <= CDF[i] over this shard's unnormalised masses
+        from oracle import sv as osv
+        return torch.as_tensor(osv.sample_cdf(vec.numpy().astype(np.complex128), uniforms.numpy()))
+
 
 def _circuit(n, seed, size):
     from quict_b200.core import Circuit, GATE_BY_NAME
@@ -76,10 +81,11 @@ def _worker(rank, world, port, n, seed, chunk, q):
         probs = [sv.prob0(qb) for qb in range(n)]  # before re-ordering: global and local bits
         norm = sv.norm2()
         ex = sv.exchanges
+        shots = sv.sample(500, uniforms=np.random.default_rng(seed + 100).random(500))
         full = sv.gather(0)
-        q.put((rank, full, probs, norm, ex, list(sv.where)))
+        q.put((rank, full, probs, norm, ex, list(sv.where), shots))
     except Exception as e:  # noqa: BLE001 - reported to the parent
-        q.put((rank, repr(e), None, None, None, None))
+        q.put((rank, repr(e), None, None, None, None, None))
     finally:
         dist.destroy_process_group()
 
@@ -106,8 +112,14 @@ def test_sharded_vector_matches_the_oracle(world, n, seed, chunk):
         assert not isinstance(res[r][0], str), res[r][0]
     c = _circuit(n, seed, 80)
     ref = osv.run(oracle_gates(c), n)
-    full, probs, norm, ex, where = res[0]
+    full, probs, norm, ex, where, shots = res[0]
     np.testing.assert_allclose(full, ref, rtol=0, atol=1e-12)
+    u = np.random.default_rng(seed + 100).random(500)
+    want = osv.sample_cdf(ref, u)
+    ties = osv.near_ties(ref, u, 1e-12)
+    assert np.all((shots == want) | ties)
+    for r in range(1, world):
+        np.testing.assert_array_equal(res[r][5], shots)  # every rank holds all shots
     assert where == list(range(n))
     assert abs(norm - 1) < 1e-12
     for qb in range(n):
@@ -174,6 +186,10 @@ def test_solo_vector_on_the_gpu_engine(cuda_ok, precision, tol):
     assert abs(sv.norm2() - 1) < 10 * tol
     want = float(np.sum(np.abs(ref[: 1 << 11]) ** 2))  # qubit 0 = vector bit 11
     assert abs(sv.prob0(0) - want) < 10 * tol
+    u = np.random.default_rng(8).random(1000)
+    shots = sv.sample(1000, uniforms=u)
+    ties = osv.near_ties(ref, u, 1e-12 if precision == "double" else 1e-5)
+    assert np.all((shots == osv.sample_cdf(ref, u)) | ties)
 
 
 def test_exchange_choice_looks_ahead():
