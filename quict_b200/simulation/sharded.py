@@ -44,13 +44,14 @@ class ShardedStateVector:
     without an initialised process group, one unsplit vector on this device.
 
     ``backend`` runs the local work on one shard: ``apply_ops(vec, n, ops)``,
-    ``prob0(vec, n, bit)`` and ``norm2(vec, n)`` -- by default the CUDA engine
-    of this package on ``device``.  ``chunk_bytes`` bounds the staging buffers
+    ``prob0(vec, n, bit)``, ``norm2(vec, n)``, ``collapse``, ``reset`` and
+    ``sample_indices`` -- by default the CUDA engine of this package on
+    ``device``.  ``chunk_bytes`` bounds the staging buffers
     of one exchange (the half-shard is sent in pieces of at most that size).
     """
 
     def __init__(self, n: int, precision: str = "double", group=None, device: Optional[torch.device] = None,
-                 backend=None, chunk_bytes: int = 1 << 28):
+                 backend=None, chunk_bytes: int = 1 << 28, seed: Optional[int] = None):
         self.group = group
         # without a process group the vector is one unsplit shard on this device
         self.solo = group is None and not dist.is_initialized()
@@ -73,6 +74,7 @@ class ShardedStateVector:
         self.chunk_bytes = int(chunk_bytes)
         self.where = list(range(n))  # logical vector bit -> physical bit
         self.exchanges = 0           # half-shard exchanges issued by this rank
+        self.rng = np.random.default_rng(seed)  # measurement draws (rank 0's are used)
         self.local = torch.zeros(1 << self.nl, dtype=self.dtype, device=self.device)
         if self.rank == 0:
             self.local[0] = 1
@@ -218,15 +220,83 @@ class ShardedStateVector:
             self._uses = None
 
     def run(self, circuit) -> "ShardedStateVector":
-        """Apply a circuit's unitary gates from the current state (|0...0> at
-        construction); measure / reset / perm gates are refused."""
+        """Apply a circuit from the current state (|0...0> at construction).
+        Measure and Reset gates act mid-circuit with the reference's rules
+        (outcomes are recorded on ``circuit.qubits[q].measured``); Perm gates
+        are refused."""
         if int(circuit.width()) != self.n:
             raise ValueError(f"circuit has {circuit.width()} qubits, the vector {self.n}")
         ops: List[Op] = []
         for g in circuit.gates:
-            ops.extend(lower_gate(g, self.n))
+            for op in lower_gate(g, self.n):
+                if op.kind in ("measure", "reset"):
+                    self.apply_ops(ops)
+                    ops = []
+                    if op.kind == "measure":
+                        circuit.qubits[op.qubit].measured = self.measure(op.qubit)
+                    else:
+                        self.reset(op.qubit)
+                else:
+                    ops.append(op)
         self.apply_ops(ops)
         return self
+
+    # ---- measurement ------------------------------------------------------------------------
+    def _shared_uniform(self) -> float:
+        """One uniform, the same on every rank (rank 0 draws it)."""
+        u = float(self.rng.random()) if self.rank == 0 else 0.0
+        if self.solo:
+            return u
+        t = torch.tensor([u], dtype=torch.float64, device=self._reduce_dev())
+        dist.broadcast(t, 0 if self.group is None else dist.get_global_rank(self.group, 0), group=self.group)
+        return float(t.item())
+
+    def measure(self, qubit: int, u: Optional[float] = None) -> int:
+        """Measure one qubit with the reference rule: outcome 1 iff u > P(0),
+        the kept half scaled by 1/sqrt(p), the other zeroed.  `u`, if given,
+        must be the same on every rank."""
+        p0 = self.prob0(qubit)
+        if u is None:
+            u = self._shared_uniform()
+        one = int(u > p0)
+        scale = 1.0 / np.sqrt((1.0 - p0) if one else p0)
+        p = self.where[self.n - 1 - qubit]
+        if p < self.nl:
+            self.backend.collapse(self.local, self.nl, p, one, scale)
+        elif self._rank_bit(p) == one:
+            self.local.mul_(scale)
+        else:
+            self.local.zero_()
+        return one
+
+    def reset(self, qubit: int):
+        """Reset one qubit to |0> with the reference rule: alpha = sqrt(P(0));
+        alpha < 1e-6 moves the |1> half into |0>, else the |0> half is divided
+        by alpha; the |1> half becomes 0.  On a rank bit the move is a whole
+        shard sent from the bit-1 rank to its bit-0 partner."""
+        p0 = self.prob0(qubit)
+        p = self.where[self.n - 1 - qubit]
+        if p < self.nl:
+            self.backend.reset(self.local, self.nl, p, p0)
+            return
+        alpha = float(np.sqrt(p0))
+        mine = self._rank_bit(p)
+        if alpha >= 1e-6:
+            if mine:
+                self.local.zero_()
+            else:
+                self.local.div_(alpha)
+            return
+        partner = self.rank ^ (1 << (p - self.nl))
+        peer = partner if self.group is None else dist.get_global_rank(self.group, partner)
+        buf = torch.view_as_real(self.local)
+        if mine:
+            dist.send(buf.contiguous(), peer, group=self.group)
+            self.local.zero_()
+        else:
+            recv = torch.empty_like(buf)
+            dist.recv(recv, peer, group=self.group)
+            self.local.copy_(torch.view_as_complex(recv))
 
     def canonical(self):
         """Bring every logical bit back to its own physical bit (exchanges for

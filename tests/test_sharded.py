@@ -49,6 +49,24 @@ class _NumpyShard:
         idx = np.arange(v.size)
         return float(np.sum(np.abs(v[(idx >> bit) & 1 == 0]) ** 2))
 
+    def collapse(self, vec, n, bit, outcome, scale):
+        v = vec.numpy()
+        idx = np.arange(v.size)
+        hit = ((idx >> bit) & 1) == outcome
+        v[hit] *= scale
+        v[~hit] = 0
+
+    def reset(self, vec, n, bit, p0):
+        v = vec.numpy()
+        idx = np.arange(v.size)
+        zero, one = idx[((idx >> bit) & 1) == 0], idx[((idx >> bit) & 1) == 1]
+        alpha = np.sqrt(p0)
+        if alpha < 1e-6:
+            v[zero] = v[one]
+        else:
+            v[zero] /= alpha
+        v[one] = 0
+
     def sample_indices(self, vec, n, uniforms, mode):
         # smallest i with u <= CDF[i] over this shard's unnormalised masses
         from oracle import sv as osv
@@ -224,3 +242,84 @@ def test_exchange_choice_looks_ahead():
         hits = sum(1 for o in ops if o.kind != "diag" and any(b >= d.nl for b in o.tbits))
         assert 0 < d.exchanges <= 2 * d.g < hits
         assert sorted(d.where) == list(range(n))
+
+
+def _mr_plan(n, seed):
+    """Segments of gates, each followed by a measure or reset of one qubit
+    (a measure is sometimes followed by a reset of the same qubit, which
+    reaches the |1> -> |0> move when the outcome was 1)."""
+    rng = np.random.default_rng(seed)
+    plan = []
+    for k in range(10):
+        seg = _circuit(n, seed * 100 + k, 12)
+        q = int(rng.integers(n))
+        plan.append((seg, "measure", q))
+        if rng.random() < 0.5:
+            plan.append((None, "reset", q))
+        else:
+            plan.append((None, "reset", int(rng.integers(n))))
+    return plan
+
+
+def _mr_worker(rank, world, port, n, seed, q):
+    import datetime
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from quict_b200.simulation.sharded import ShardedStateVector
+        sv = ShardedStateVector(n, "double", backend=_NumpyShard(), seed=seed)
+        log = []
+        for seg, what, qb in _mr_plan(n, seed):
+            if seg is not None:
+                sv.run(seg)
+            on_rank_bit = sv.where[n - 1 - qb] >= sv.nl
+            if what == "measure":
+                log.append(("measure", qb, sv.measure(qb), on_rank_bit))
+            else:
+                sv.reset(qb)
+                log.append(("reset", qb, None, on_rank_bit))
+        q.put((rank, sv.gather(0), log))
+    except Exception as e:  # noqa: BLE001 - reported to the parent
+        q.put((rank, repr(e), None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n,seed", [(2, 5, 11), (4, 6, 12)])
+def test_midcircuit_measure_and_reset_across_ranks(world, n, seed):
+    from conftest import oracle_gates
+    from oracle import sv as osv
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_mr_worker, args=(r, world, port, n, seed, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in procs:
+        r = q.get(timeout=180)
+        res[r[0]] = r[1:]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    full, log = res[0]
+    assert not isinstance(full, str), full
+    # replay with the oracle and rank 0's uniform stream
+    rng = np.random.default_rng(seed)
+    v = osv.zero_state(n)
+    for (seg, what, qb), (w2, q2, outcome, _) in zip(_mr_plan(n, seed), log):
+        assert (what, qb) == (w2, q2)
+        if seg is not None:
+            v = osv.run(oracle_gates(seg), n, vec=v)
+        if what == "measure":
+            v, one = osv.measure(v, n, qb, float(rng.random()))
+            assert one == outcome
+        else:
+            v = osv.reset(v, n, qb)
+    np.testing.assert_allclose(full, v, rtol=0, atol=1e-12)
+    assert any(flag for *_, flag in log) and not all(flag for *_, flag in log)  # both paths ran
+    for r in range(1, world):
+        assert res[r][1] == log
