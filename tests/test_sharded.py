@@ -208,6 +208,12 @@ def test_solo_vector_on_the_gpu_engine(cuda_ok, precision, tol):
     shots = sv.sample(1000, uniforms=u)
     ties = osv.near_ties(ref, u, 1e-12 if precision == "double" else 1e-5)
     assert np.all((shots == osv.sample_cdf(ref, u)) | ties)
+    # mid-circuit measure (given uniform) and reset through the engine's kernels
+    ref, one = osv.measure(ref, 12, 3, 0.37)
+    assert sv.measure(3, 0.37) == one
+    ref = osv.reset(ref, 12, 5)
+    sv.reset(5)
+    np.testing.assert_allclose(sv.gather(), ref, rtol=0, atol=10 * tol)
 
 
 def test_exchange_choice_looks_ahead():
