@@ -255,17 +255,23 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bi
             continue
         # merge the hit blocks (disjoint, commuting) and the op into one block
         bits: Tuple[int, ...] = ()
-        u = np.eye(1, dtype=np.complex128)
+        u = None  # the first factor is taken as is (no product with an identity)
         srcs: List[Op] = []
         for b in hit:
-            nb = bits + tuple(x for x in b[0] if x not in bits)
-            u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
-            bits = nb
+            if u is None:
+                bits, u = b[0], b[1]
+            else:
+                nb = bits + tuple(x for x in b[0] if x not in bits)
+                u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
+                bits = nb
             srcs += b[2]
             blocks.remove(b)
         ob, ou = _full_matrix(op)
-        nb = bits + tuple(x for x in ob if x not in bits)
-        u = _embed(ou, ob, nb) @ _embed(u, bits, nb)
+        if u is None:
+            nb, u = ob, ou
+        else:
+            nb = bits + tuple(x for x in ob if x not in bits)
+            u = _embed(ou, ob, nb) @ _embed(u, bits, nb)
         blocks.append([nb, u, srcs + [op], as_diag])
     for b in list(blocks):
         close(b)
