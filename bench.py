@@ -439,11 +439,29 @@ def sweep_bytes(name, bits, n, esize):
     return int(2 * (1 << n) * esize * frac)
 
 
+def _sweep_bits(n):
+    """Target vector bits of the 1q sweep: in-warp (0, 1, 2, 4), the first
+    pair-indexed bit (5), middle (10, 20) and the highest."""
+    return [(b,) for b in sorted({0, 1, 2, 4, 5, 10, 20, n - 1}) if b < n]
+
+
+def _sweep_pairs(n):
+    """(first, second) vector bits of the 2q sweep: both in-warp, mixed, both
+    high, and the highest with the lowest."""
+    cand = [(1, 0), (4, 2), (10, 5), (20, 10), (n - 1, n - 2), (n - 1, 0)]
+    out = []
+    for p in cand:
+        if max(p) < n and p[0] != p[1] and p not in out:
+            out.append(p)
+    return out
+
+
 def gate_sweep(eng, vec, n, ws, reps=5, warmup=2):
     """Single-gate sweep: each gate class of the config-1 gate set applied by
-    its per-gate kernel to the resident n-qubit state at a low (in-warp), a
-    middle and the highest vector bit; device-timed per launch; GB/s from
-    ``sweep_bytes`` against the measured HBM copy bandwidth."""
+    its per-gate kernel to the resident n-qubit state at vector bits from the
+    in-warp ones to the highest (``_sweep_bits`` / ``_sweep_pairs``);
+    device-timed per launch; GB/s from ``sweep_bytes`` against the measured
+    HBM copy bandwidth."""
     import torch
     from quict_b200.core import GATE_BY_NAME
     from quict_b200.simulation.lowering import lower_gate
@@ -456,7 +474,7 @@ def gate_sweep(eng, vec, n, ws, reps=5, warmup=2):
             g = g(*[0.3 + 0.1 * i for i in range(g.params)])
         two = name in SWEEP_2Q
         # (vector bits) -> circuit qubits (qubit q is vector bit n-1-q)
-        for bits in ([(1, 0), (14, 3), (n - 1, n - 2)] if two else [(0,), (14,), (n - 1,)]):
+        for bits in (_sweep_pairs(n) if two else _sweep_bits(n)):
             (op,) = lower_gate(g & [n - 1 - b for b in bits], n)
             for _ in range(warmup):
                 eng.apply_single(vec, n, op)
