@@ -65,3 +65,39 @@ def test_peak_source_and_plan_of_the_bench_circuit():
     steps = plan(ops, n, 11, 5, merge_bits=2)
     passes = [s for s in steps if isinstance(s, Pass)]
     assert passes and all(bench.pass_flops(p, n) > 0 for p in passes)
+
+
+def _max_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench as b
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        b.barrier(world)
+        q.put((rank, b.max_over_ranks(1.5 + rank, world)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_with_two_gloo_ranks():
+    """The timing reduction every multi-rank bench line uses: the max over ranks."""
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_max_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert res == {0: 2.5, 1: 2.5}
+    assert bench.max_over_ranks(3.25, 1) == 3.25
