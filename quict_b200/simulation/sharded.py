@@ -107,6 +107,9 @@ class ShardedStateVector:
         # pieces of at most chunk_bytes: whole rows when a row fits, else column blocks
         cstep = max(1, min(cols, self.chunk_bytes // per_elem))
         rstep = max(1, self.chunk_bytes // (cols * per_elem)) if cstep == cols else 1
+        # two pieces in flight: piece k+1 is on the wire while piece k is
+        # written back into the shard
+        inflight = None
         for r0 in range(0, rows, rstep):
             for c0 in range(0, cols, cstep):
                 part = half[r0:r0 + rstep, c0:c0 + cstep]
@@ -115,11 +118,21 @@ class ShardedStateVector:
                 recv = torch.empty_like(send)
                 reqs = dist.batch_isend_irecv([dist.P2POp(dist.isend, send, peer, self.group),
                                                dist.P2POp(dist.irecv, recv, peer, self.group)])
-                for q in reqs:
-                    q.wait()
-                part.copy_(torch.view_as_complex(recv))
+                if inflight is not None:
+                    self._land(*inflight)
+                inflight = (reqs, part, recv, send)
+        if inflight is not None:
+            self._land(*inflight)
         self._swap_roles(gbit, lbit)
         self.exchanges += 1
+
+    @staticmethod
+    def _land(reqs, part, recv, send):
+        """Wait for one piece's send/recv pair and write the received data
+        into its place (`send` is kept alive until its send completed)."""
+        for q in reqs:
+            q.wait()
+        part.copy_(torch.view_as_complex(recv))
 
     # ---- placing one op -----------------------------------------------------------------
     def _free_local(self, busy: set, at: int = -1) -> int:
