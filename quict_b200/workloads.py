@@ -84,24 +84,71 @@ def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int =
     return circ, obs, params
 
 
+def sharded_run(qubits: int, precision: str, gates: int, seed: int = 1) -> dict:
+    """The config-1 style circuit on a vector sharded over every rank of the
+    default process group (one GPU per rank, NCCL), device-timed with CUDA
+    events and reduced as the max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from .simulation.sharded import ShardedStateVector
+    circuit = config1_circuit(qubits, gates, seed)
+    sv = ShardedStateVector(qubits, precision, device=torch.device("cuda", torch.cuda.current_device()))
+    sv.run(config1_circuit(qubits, 8, seed + 1))  # warm-up: knobs, matrix tables, communicators
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ex0 = sv.exchanges
+    e0.record()
+    sv.run(circuit)
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return {"workload": f"sv-{qubits}q-{precision}-{gates}g-config1 sharded over {sv.world} ranks",
+            "ms": ms, "gates_per_s": gates / (ms / 1e3), "exchanges": sv.exchanges - ex0,
+            "norm2": sv.norm2()}
+
+
 def main() -> None:
-    """Run one workload on cuda:0 (for profiling a single kernel family):
+    """Run one workload (for profiling a single kernel family):
 
         python -m quict_b200.workloads gradient --batch 256 [--precision single] [--repeat 2]
-            [--tile-bits K] [--pair-tile-bits K]
+            [--tile-bits K] [--pair-tile-bits K]                       (cuda:0)
+        torchrun --nproc-per-node N -m quict_b200.workloads sharded --qubits Q
+            [--precision double] [--gates 1000]                        (one GPU per rank)
     """
     import argparse
+    import json
+    import os
 
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["gradient"])
+    ap.add_argument("workload", choices=["gradient", "sharded"])
     ap.add_argument("--batch", type=int, default=1024)
-    ap.add_argument("--precision", default="single", choices=["single", "double"])
+    ap.add_argument("--precision", default=None, choices=["single", "double"])
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--tile-bits", type=int, default=None, help="forward register tile width k")
     ap.add_argument("--pair-tile-bits", type=int, default=None, help="backward pair tile width k")
+    ap.add_argument("--qubits", type=int, default=32)
+    ap.add_argument("--gates", type=int, default=1000)
     a = ap.parse_args()
+    if a.workload == "sharded":
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            res = sharded_run(a.qubits, a.precision or "double", a.gates)
+            if dist.get_rank() == 0:
+                print(json.dumps(res))
+        finally:
+            dist.destroy_process_group()
+        return
+    a.precision = a.precision or "single"
     from .differentiation import BatchedAdjoint
     circ, obs, params = config3_problem(16, 8, a.batch)
     eng = BatchedAdjoint(circ, obs, a.precision, tile_bits=a.tile_bits, pair_tile_bits=a.pair_tile_bits)
