@@ -236,6 +236,17 @@ def test_abi_validation_without_gpu():
     ops[0].gbit[0], ops[0].tgt[0] = 5, 2
     ops[0].mat = 1  # 4 entries needed from offset 1 in a 4-entry table
     assert lib.qs_apply_fused(fake, 8, N.QS_C128, ps, 1, ops, 1, fake, 4, None) == N.QS_EINVAL
+    # adjoint pair passes: every case below fails validation before any device access
+    assert lib.qs_adjoint_pair(None, 10, N.QS_C64, ps, 1, ops, 1, fake, 4, fake, 2, None) == N.QS_EINVAL
+    assert lib.qs_adjoint_pair(fake, 1, N.QS_C64, ps, 1, ops, 1, fake, 4, fake, 2, None) == N.QS_EINVAL
+    assert b"bit count" in lib.qs_last_error()
+    assert lib.qs_adjoint_pair(fake, 10, 7, ps, 1, ops, 1, fake, 4, fake, 2, None) == N.QS_EINVAL
+    assert lib.qs_adjoint_pair(fake, 10, N.QS_C64, None, 1, ops, 1, fake, 4, fake, 2, None) == N.QS_EINVAL
+    # a register tile needs nlow >= 5 and k - R in [5, 8]: a 2^3 tile is refused
+    ops[0].mat = 0
+    ps[0].pair = 8
+    assert lib.qs_adjoint_pair(fake, 8, N.QS_C64, ps, 1, ops, 1, fake, 4, fake, 2, None) == N.QS_EINVAL
+    assert b"register tile" in lib.qs_last_error() or b"pair" in lib.qs_last_error()
 
 
 def test_merge_ops_reduces_op_count_and_keeps_kinds():
