@@ -325,3 +325,40 @@ def test_merged_blocks_act_like_the_ops(seed):
         return v
 
     np.testing.assert_allclose(run(merged), run(ops), atol=1e-12)
+
+
+def test_planner_property_random_circuits_and_knobs():
+    """Property check over random circuits and planner knobs: the passes keep
+    every op's non-diagonal bits inside their tile, never exceed the op or
+    matrix-table limits, and act like the circuit (FP64 oracle)."""
+    from hypothesis import given, settings, strategies as st, HealthCheck
+    from quict_b200 import _native as N
+    from quict_b200.core import Circuit
+    from quict_b200.simulation.fusion import Pass, iter_plan, op_entries, relabel_swaps
+    from quict_b200.simulation.lowering import lower_circuit
+
+    @settings(max_examples=40, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+    @given(n=st.integers(2, 7), seed=st.integers(0, 10 ** 6), size=st.integers(0, 60),
+           k=st.integers(1, 12), nlow=st.integers(0, 6), merge=st.sampled_from([0, 2, 3]),
+           max_ops=st.integers(1, 40))
+    def check(n, seed, size, k, nlow, merge, max_ops):
+        c = Circuit(n)
+        if size:
+            c.random_append(size, seed=seed)
+        ops = lower_circuit(c.gates, n)
+        flat = []
+        for s in iter_plan(relabel_swaps(ops, n), n, k, nlow, max_ops=max_ops, merge_bits=merge):
+            if isinstance(s, Pass):
+                tile = set(range(min(nlow, k, n))) | set(s.hi)
+                assert len(tile) == min(k, n)
+                assert len(s.ops) <= max(max_ops, 1)
+                assert sum(op_entries(o) for o in s.ops) <= N.QS_MAX_PASS_MATS
+                for o in s.ops:
+                    assert o.xbits <= tile
+                flat.extend(s.ops)
+            else:
+                flat.append(s.op)
+        ref = osv.run(oracle_gates(c), n) if size else osv.zero_state(n)
+        np.testing.assert_allclose(_apply_ops_oracle(osv.zero_state(n), n, flat), ref, atol=1e-12)
+
+    check()
