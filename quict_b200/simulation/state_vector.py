@@ -213,11 +213,13 @@ class StateVectorSimulator:
         return int(one)
 
     # ---- reference helpers ---------------------------------------------------------------
-    def get_measured_prob(self, index: int, all_measured: bool = False) -> float:
-        """P(vector bit `index` = 0) in FP64 (all_measured: total norm)."""
+    def get_measured_prob(self, index: int, all_measured: bool = False) -> "MeasuredProb":
+        """P(vector bit `index` = 0) in FP64 (all_measured: total norm).  A
+        float that also has QuICT's ``.get()`` (its GPU path returns a device
+        scalar that callers read with ``.get()``)."""
         if all_measured:
-            return self._engine.norm2(self._vector, self._qubits)
-        return self._engine.prob0(self._vector, self._qubits, index)
+            return MeasuredProb(self._engine.norm2(self._vector, self._qubits))
+        return MeasuredProb(self._engine.prob0(self._vector, self._qubits, index))
 
     def apply_specialgate(self, index: int, type, prob: float = None):
         name = getattr(type, "name", type)
@@ -278,6 +280,13 @@ class StateVectorSimulator:
         if not return_counts:
             return idx
         return self._engine.counts_list(idx, 1 << n)
+
+
+class MeasuredProb(float):
+    """A probability read back from the device: a float with ``.get()``."""
+
+    def get(self) -> float:
+        return float(self)
 
 
 def _is_trigger(g) -> bool:

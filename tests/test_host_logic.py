@@ -362,3 +362,10 @@ def test_planner_property_random_circuits_and_knobs():
         np.testing.assert_allclose(_apply_ops_oracle(osv.zero_state(n), n, flat), ref, atol=1e-12)
 
     check()
+
+
+def test_measured_prob_is_a_float_with_get():
+    """get_measured_prob returns a float that also answers QuICT's ``.get()``."""
+    from quict_b200.simulation.state_vector import MeasuredProb
+    p = MeasuredProb(0.375)
+    assert isinstance(p, float) and p.get() == 0.375 and p * 2 == 0.75 and type(p.get()) is float
