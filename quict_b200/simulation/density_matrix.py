@@ -166,6 +166,29 @@ class DensityMatrixSimulator:
                     pending.append(op)
         self._engine.apply_ops(vec, 2 * n, pending)
 
+    def apply_gates(self, cgate):
+        """rho <- M rho M^dagger for the unitary gates of a composite gate (or
+        any iterable of gates / object with ``.gates``), as the reference's
+        ``apply_gates`` (density_matrix_simulator.py:147-159) does with the
+        composite's full matrix; here each gate is a local update."""
+        gates = getattr(cgate, "gates", cgate)
+        n = self._qubits
+        ops: List[Op] = []
+        for g in gates:
+            for op in lower_dm(g, n):
+                if op.kind in ("measure", "reset", "perm"):
+                    raise TypeError(f"apply_gates takes unitary gates only, not {op.kind}")
+                ops.append(op)
+        self._engine.apply_ops(self._density_matrix.view(-1), 2 * n, ops)
+
+    def apply_noise(self, noise_gate, qubits: int):
+        """rho <- sum_K K rho K^dagger for a NoiseGate's Kraus set on its
+        targets (density_matrix_simulator.py:161-180); `qubits` is the
+        circuit's qubit count, as in the reference."""
+        if int(qubits) != self._qubits:
+            raise ValueError(f"apply_noise: {qubits} qubits given, the density matrix has {self._qubits}")
+        self._engine.apply_ops(self._density_matrix.view(-1), 2 * self._qubits, lower_dm(noise_gate, self._qubits))
+
     def apply_measure(self, qubit: int, u: Optional[float] = None) -> int:
         """Reference rule (density_matrix_simulator.py:182-208): P(0) = trace of the
         projected diagonal; outcome 1 iff u > P(0); rho <- P rho P / p."""

@@ -43,6 +43,11 @@ class UnitarySimulator:
     def vector(self, vec):
         self._vector = torch.as_tensor(np.asarray(vec), dtype=self._tdtype).to(self._tdev)
 
+    def initial_vector_state(self):
+        """|0...0> of the current qubit count (unitary_simulator.py:49-57)."""
+        self._vector = torch.zeros(1 << self._qubits_num, dtype=self._tdtype, device=self._tdev)
+        self._vector[0] = 1
+
     def get_unitary_matrix(self, circuit) -> StateArray:
         n = int(circuit.width())
         if n > self.MAX_QUBITS:

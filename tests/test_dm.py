@@ -181,3 +181,29 @@ def test_dm_measure_and_sample(cuda_ok):
 def oracle_gates_unitary(c):
     return [(np.asarray(g.matrix, dtype=np.complex128), list(g.cargs) + list(g.targs))
             for g in c.gates if g.type.name not in ("measure",)]
+
+
+@pytest.mark.gpu
+def test_dm_apply_gates_and_apply_noise(cuda_ok):
+    """The reference's public step methods: apply_gates (a composite / gate
+    list) and apply_noise (a NoiseGate's Kraus set), against the oracle."""
+    from quict_b200.core import CX, H, Rz, Circuit, DampingError, DepolarizingError
+    from quict_b200.core.noise import NoiseGate
+    from quict_b200.simulation import DensityMatrixSimulator
+    n = 3
+    c = Circuit(n)
+    c.random_append(20, seed=3)
+    sim = DensityMatrixSimulator("GPU")
+    sim.run(c)
+    rho = odm.run(oracle_gates(c), n)
+    gates = [H & 0, CX & [0, 2], Rz(0.4) & 1]
+    sim.apply_gates(gates)
+    rho = odm.run([(np.asarray(g.matrix), list(g.cargs) + list(g.targs)) for g in gates], n, rho=rho)
+    err = DampingError(amplitude_prob=0.1, phase_prob=0).compose(DepolarizingError(0.05, 1))
+    ng = NoiseGate(err.apply_to_gate_array(np.eye(2)), 1)
+    ng.targs = [1]
+    sim.apply_noise(ng, n)
+    rho = odm.apply_channel(rho, n, [np.asarray(k) for k in ng.noise_matrix], [1])
+    np.testing.assert_allclose(sim.density_matrix.get(), rho, rtol=0, atol=1e-12)
+    with pytest.raises(ValueError):
+        sim.apply_noise(ng, n + 1)

@@ -103,3 +103,16 @@ def test_unitary_simulator_vs_oracle(cuda_ok, precision, tol):
     np.testing.assert_allclose(u, ref, atol=tol * 10)
     counts = sim.sample(100, seed=1)
     assert sum(counts) == 100
+
+
+@pytest.mark.gpu
+def test_unitary_initial_vector_state(cuda_ok):
+    from quict_b200.core import Circuit
+    from quict_b200.simulation.unitary import UnitarySimulator
+    c = Circuit(4)
+    c.random_append(20, seed=4)
+    sim = UnitarySimulator("GPU")
+    sim.run(c)
+    sim.initial_vector_state()
+    v = sim.vector.get()
+    assert v.shape == (16,) and v[0] == 1 and np.count_nonzero(v) == 1
