@@ -134,6 +134,11 @@ class Circuit:
         for q in self._qubits:
             q.measured = None
 
+    def qasm(self) -> str:
+        """OpenQASM 2.0 text of the circuit (QuICT's ``Circuit.qasm``)."""
+        from .qasm import dumps
+        return dumps(self)
+
     def random_append(self, rand_size: int = 10, typelist: Optional[list] = None, random_params: bool = True,
                       seed: Optional[int] = None):
         """Append `rand_size` gates drawn uniformly from `typelist` on distinct random qubits.

@@ -59,9 +59,8 @@ class Result:
     def record_circuit(self, circuit):
         self.id = getattr(circuit, "name", None) or self.id
         if self._circuit_record:
-            from ..core.qasm import dumps
             with open(os.path.join(self._output_path, f"circuit_{self.id}.qasm"), "w") as f:
-                f.write(dumps(circuit))
+                f.write(circuit.qasm())
 
     def record_amplitude(self, amplitude):
         a = amplitude.get() if hasattr(amplitude, "get") else np.asarray(amplitude)

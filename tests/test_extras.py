@@ -116,3 +116,14 @@ def test_unitary_initial_vector_state(cuda_ok):
     sim.initial_vector_state()
     v = sim.vector.get()
     assert v.shape == (16,) and v[0] == 1 and np.count_nonzero(v) == 1
+
+
+def test_circuit_qasm_method_round_trips():
+    from quict_b200.core import Circuit
+    from quict_b200.core.qasm import loads
+    c = Circuit(4)
+    c.random_append(30, seed=8)
+    c2 = loads(c.qasm())
+    assert [g.type.name for g in c2.gates] == [g.type.name for g in c.gates]
+    assert [list(g.cargs) + list(g.targs) for g in c2.gates] == [list(g.cargs) + list(g.targs) for g in c.gates]
+    np.testing.assert_allclose(osv.run(oracle_gates(c2), 4), osv.run(oracle_gates(c), 4), atol=1e-12)
