@@ -76,7 +76,7 @@ class DensityMatrixSimulator:
                  gpu_device_id: int = 0, fusion: bool = True, tile_bits: Optional[int] = None,
                  low_bits: Optional[int] = None, merge_bits: Optional[int] = None, seed=None):
         if device != "GPU":
-            raise ValueError(f"DensityMatrixSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
+            raise ValueError(f"DensityMatrixSimulator.device must be 'GPU' (quict_b200 has no CPU path), got {device!r}")
         if precision not in ("single", "double"):
             raise ValueError("DensityMatrixSimulator.precision must be 'single' or 'double'")
         self._precision = np.complex128 if precision == "double" else np.complex64

@@ -3,7 +3,7 @@ over this package's GPU simulators, with its result record
 (QuICT/simulation/utils/result.py:5-110).
 
 Same constructor, option table, argument checks and result dictionary; the
-device must be "GPU" (this build has no CPU path).  ``run`` runs the circuit,
+device must be "GPU" (quict_b200 has no CPU path).  ``run`` runs the circuit,
 samples ``shots`` times and returns the record: counts keyed by the
 zero-padded bit string of every basis index (zeros included, as QuICT does),
 and the amplitudes / density matrix as numpy arrays.
@@ -99,7 +99,7 @@ class Simulator:
         if device not in self.__DEVICE:
             raise ValueError(f"Simulator.device must be one of {self.__DEVICE}, got {device!r}")
         if device != "GPU":
-            raise ValueError("Simulator.device must be 'GPU' (this build has no CPU path)")
+            raise ValueError("Simulator.device must be 'GPU' (quict_b200 has no CPU path)")
         if backend not in self.__BACKEND:
             raise ValueError(f"Simulator.backend must be one of {self.__BACKEND}, got {backend!r}")
         if precision not in self.__PRECISION:

@@ -72,7 +72,7 @@ class StateVectorSimulator:
                  max_pass_cost: Optional[float] = None, merge_bits: Optional[int] = None,
                  legacy_2q_order: bool = False, seed: Optional[int] = None, autotune: bool = False):
         if device not in self.__DEVICE:
-            raise ValueError(f"StateVectorSimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
+            raise ValueError(f"StateVectorSimulator.device must be 'GPU' (quict_b200 has no CPU path), got {device!r}")
         if precision not in self.__PRECISION:
             raise ValueError(f"StateVectorSimulator.precision must be one of {self.__PRECISION}, got {precision!r}")
         self._device = device

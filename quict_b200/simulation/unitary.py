@@ -25,7 +25,7 @@ class UnitarySimulator:
 
     def __init__(self, device: str = "GPU", precision: str = "double", *, gpu_device_id: int = 0, seed=None):
         if device != "GPU":
-            raise ValueError(f"UnitarySimulator.device must be 'GPU' (this build has no CPU path), got {device!r}")
+            raise ValueError(f"UnitarySimulator.device must be 'GPU' (quict_b200 has no CPU path), got {device!r}")
         self._precision = np.complex128 if precision == "double" else np.complex64
         self._tdtype = torch.complex128 if precision == "double" else torch.complex64
         self._tdev = require_cuda(gpu_device_id)

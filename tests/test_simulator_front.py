@@ -12,7 +12,7 @@ def test_argument_checks_before_any_device():
     with pytest.raises(ValueError):
         Simulator("TPU")
     with pytest.raises(ValueError):
-        Simulator("CPU")  # this build has no CPU path
+        Simulator("CPU")  # quict_b200 has no CPU path
     with pytest.raises(ValueError):
         Simulator("GPU", backend="tensor_network")
     with pytest.raises(ValueError):
