@@ -92,7 +92,7 @@ def test_max_over_ranks_with_two_gloo_ranks():
     s.close()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_max_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_max_worker, args=(r, 2, port, q), daemon=True) for r in range(2)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=120) for _ in procs)

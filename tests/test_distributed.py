@@ -55,7 +55,7 @@ def test_sharded_energies_gather_in_order():
     world, port = 2, _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_energies_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_energies_worker, args=(r, world, port, q), daemon=True) for r in range(world)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=120) for _ in procs)
@@ -102,7 +102,7 @@ def test_failed_rank_is_detected_by_timeout():
     world, port = 2, _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, q), daemon=True) for r in range(world)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=120) for _ in procs)

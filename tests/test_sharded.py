@@ -117,7 +117,7 @@ def test_sharded_vector_matches_the_oracle(world, n, seed, chunk, precision):
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, n, seed, chunk, q, precision)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, n, seed, chunk, q, precision), daemon=True) for r in range(world)]
     for p in procs:
         p.start()
     res = {}
@@ -303,7 +303,7 @@ def test_midcircuit_measure_and_reset_across_ranks(world, n, seed):
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_mr_worker, args=(r, world, port, n, seed, q)) for r in range(world)]
+    procs = [ctx.Process(target=_mr_worker, args=(r, world, port, n, seed, q), daemon=True) for r in range(world)]
     for p in procs:
         p.start()
     res = {}
