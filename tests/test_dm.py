@@ -207,3 +207,38 @@ def test_dm_apply_gates_and_apply_noise(cuda_ok):
     np.testing.assert_allclose(sim.density_matrix.get(), rho, rtol=0, atol=1e-12)
     with pytest.raises(ValueError):
         sim.apply_noise(ng, n + 1)
+
+
+class _NumpyEngine:
+    """Applies lowered ops on a CPU tensor with the oracle (host-logic check)."""
+
+    def apply_ops(self, vec, n, ops):
+        v = vec.numpy()
+        out = _apply_dm_ops(v.reshape(1 << (n // 2), 1 << (n // 2)), n // 2, ops).reshape(-1)
+        v[:] = out
+
+
+def test_dm_step_methods_host_logic():
+    """apply_gates / apply_noise lower to the ops the oracle expects (the ops
+    are applied by a numpy stand-in here; the GPU test runs the kernels)."""
+    import torch
+    from quict_b200.core import CX, H, Rz, DampingError, DepolarizingError
+    from quict_b200.core.noise import NoiseGate
+    from quict_b200.simulation import DensityMatrixSimulator
+    n = 3
+    sim = DensityMatrixSimulator.__new__(DensityMatrixSimulator)
+    sim._qubits = n
+    sim._density_matrix = torch.from_numpy(odm.zero_dm(n).copy())
+    sim._engine = _NumpyEngine()
+    gates = [H & 0, CX & [0, 2], Rz(0.4) & 1]
+    sim.apply_gates(gates)
+    rho = odm.run([(np.asarray(g.matrix), list(g.cargs) + list(g.targs)) for g in gates], n)
+    err = DampingError(amplitude_prob=0.1, phase_prob=0).compose(DepolarizingError(0.05, 1))
+    ng = NoiseGate(err.apply_to_gate_array(np.eye(2)), 1)
+    ng.targs = [1]
+    sim.apply_noise(ng, n)
+    rho = odm.apply_channel(rho, n, [np.asarray(k) for k in ng.noise_matrix], [1])
+    np.testing.assert_allclose(sim._density_matrix.numpy(), rho, rtol=0, atol=1e-12)
+    with pytest.raises(TypeError):
+        from quict_b200.core import Measure
+        sim.apply_gates([Measure & 0])
