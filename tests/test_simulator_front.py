@@ -64,3 +64,44 @@ def test_simulator_runs_each_backend(cuda_ok):
     res = Simulator("GPU", "unitary", "double").run(c, shots=50)
     np.testing.assert_allclose(res["data"]["state_vector"], ref, rtol=0, atol=1e-12)
     assert res["shots"] == 50
+
+
+def test_run_flow_with_a_stand_in_backend():
+    """Simulator.run's checks, record and sampling order, with a stand-in
+    backend (the GPU test runs the real ones)."""
+    from quict_b200.core import Circuit, H
+    from quict_b200.simulation import Result, Simulator, SimulatorOptionsUnmatchedError
+
+    class Fake:
+        def __init__(self):
+            self.calls = []
+
+        def run(self, *args):
+            self.calls.append(("run", args[1:]))
+            return np.array([0.6, 0.8], dtype=np.complex128)
+
+        def sample(self, shots):
+            self.calls.append(("sample", shots))
+            return [shots - 1, 1]
+
+    for backend in ("state_vector", "density_matrix", "unitary"):
+        s = Simulator.__new__(Simulator)
+        s._device, s._backend, s._precision, s._options = "GPU", backend, "double", {}
+        s._simulator = Fake()
+        s._result_recorder = Result("GPU", backend, "double", False, False, {})
+        c = Circuit(1)
+        H | c(0)
+        res = s.run(c, shots=10)
+        assert res["shots"] == 10 and res["data"]["counts"] == {"0": 9, "1": 1}
+        key = "density_matrix" if backend == "density_matrix" else "state_vector"
+        np.testing.assert_allclose(res["data"][key], [0.6, 0.8])
+        assert [k for k, _ in s._simulator.calls] == ["run", "sample"]
+        if backend != "density_matrix":
+            with pytest.raises(SimulatorOptionsUnmatchedError):
+                s.run(c, noise_model=object())
+        else:
+            with pytest.raises(SimulatorOptionsUnmatchedError):
+                s.run(c, state_vector=np.ones(2))
+        if backend != "unitary":
+            with pytest.raises(SimulatorOptionsUnmatchedError):
+                s.run(np.eye(2))
