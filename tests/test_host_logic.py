@@ -369,3 +369,19 @@ def test_measured_prob_is_a_float_with_get():
     from quict_b200.simulation.state_vector import MeasuredProb
     p = MeasuredProb(0.375)
     assert isinstance(p, float) and p.get() == 0.375 and p * 2 == 0.75 and type(p.get()) is float
+
+
+def test_counts_list_sparse_and_dense_conversion():
+    """Engine.counts_list: the nonzero-bin path and the full-list path give the
+    same list (histogram replaced by a CPU bincount here)."""
+    import torch
+    from quict_b200.simulation.engine import Engine
+    eng = Engine.__new__(Engine)
+    eng.histogram = lambda idx, n: torch.bincount(idx, minlength=n)
+    rng = np.random.default_rng(2)
+    for ncounts, shots in ((4096, 100), (16, 1000), (1 << 12, 0), (8, 2)):
+        idx = torch.as_tensor(rng.integers(0, ncounts, shots), dtype=torch.int64)
+        got = eng.counts_list(idx, ncounts)
+        assert isinstance(got, list) and len(got) == ncounts and sum(got) == shots
+        assert got == np.bincount(idx.numpy(), minlength=ncounts).tolist()
+        assert all(type(c) is int for c in got[:4])
