@@ -19,7 +19,9 @@ roofline  the fused-pass kernel (k_fused_reg), bound fp64: algorithmic flops of
 single_gate_sweep, c64, configs_0_2, adjoint, qaoa  extra sections: per-gate HBM
         fractions, complex64 at 30/32 qubits, configs 0 and 2, gradients, QAOA batch.
 cpu_baseline  the numba port of the reference CPU kernels (oracle/ref_port.py)
-        on this host's cores, on the first gates of the same circuit.
+        on this host's cores: gates of every class of the same circuit timed,
+        rate = 1000 / sum over classes (count x mean s/gate);
+        cpu_baseline_1thread: the same on one thread (26 qubits, scaled).
 """
 from __future__ import annotations
 
@@ -144,42 +146,76 @@ def max_over_ranks(x, ws):
 
 class CpuBaseline:
     """Numba port of the reference CPU kernels (oracle/ref_port.py) on a host
-    copy of the state; the state is allocated once and reused across steps."""
+    copy of the state; the state is allocated once and reused.
 
-    def __init__(self, circuit, n):
+    Estimator: the circuit's gates are grouped by class (gate type; 2-qubit
+    Haar unitaries are "unitary").  A sample times whole gates of every class
+    in turn; the full circuit's time is estimated as sum over classes of
+    (gates of that class) x (mean sampled seconds per gate of that class), and
+    the rate is gates / that time -- total gates over total time, with each
+    class weighted by its share of the circuit."""
+
+    def __init__(self, circuit, n, threads=None):
         import numpy as np
         from oracle import ref_port
-        from quict_b200.simulation.lowering import lower_circuit
-        self.np, self.port = np, ref_port
-        self.ops = lower_circuit(circuit.gates, n)
-        self.prepared = [ref_port.prepare([op], np.complex128)[0] for op in self.ops]
+        from quict_b200.simulation.lowering import lower_gate
+        if threads is not None:
+            import numba
+            numba.set_num_threads(int(threads))
+        self.np, self.port, self.n = np, ref_port, n
+        self.classes = {}
+        self.prepared = []
+        for g in circuit.gates:
+            ops = lower_gate(g, n)
+            self.classes.setdefault(g.type.name, []).append(len(self.prepared))
+            self.prepared.append(ref_port.prepare(ops, np.complex128))
+        self.total = len(self.prepared)
         self.vec = np.zeros(1 << n, dtype=np.complex128)
         self.vec[0] = 1
+        self.times = {c: [] for c in self.classes}
         # compile every kernel signature once on a 10-qubit vector
         warm = np.zeros(1 << 10, dtype=np.complex128)
         seen = set()
-        for op in self.ops:
-            key = (op.kind, op.m, len(op.cbits))
-            if key in seen:
-                continue
-            seen.add(key)
-            t = tuple(range(op.m))
-            c = tuple(range(op.m, op.m + len(op.cbits)))
-            op2 = type(op)(op.kind, t, c, op.mat)
-            ref_port.run(warm, ref_port.prepare([op2], np.complex128))
+        for ops in (lower_gate(g, n) for g in circuit.gates):
+            for op in ops:
+                key = (op.kind, op.m, len(op.cbits))
+                if key in seen:
+                    continue
+                seen.add(key)
+                t = tuple(range(op.m))
+                c = tuple(range(op.m, op.m + len(op.cbits)))
+                ref_port.run(warm, ref_port.prepare([type(op)(op.kind, t, c, op.mat)], np.complex128))
 
-    def step(self, start, budget_s, max_gates):
-        """Apply gates from index `start`; return (gates/s, gates done, seconds)."""
-        import numba  # noqa: F401
-        done, t0 = 0, time.perf_counter()
-        for i in range(start, min(start + max_gates, len(self.ops))):
-            fn, a = self.prepared[i]
-            fn(self.vec, *a)
-            done += 1
-            if time.perf_counter() - t0 > budget_s:
-                break
-        dt = time.perf_counter() - t0
-        return done / dt, done, dt
+    def sample(self, rounds=1, budget_s=float("inf"), record=True):
+        """Time `rounds` gates of every class (the next unsampled occurrences);
+        stops early after `budget_s` seconds.  Returns seconds spent."""
+        t_all = time.perf_counter()
+        for _ in range(rounds):
+            for c, idx in self.classes.items():
+                k = idx[len(self.times[c]) % len(idx)]
+                t0 = time.perf_counter()
+                self.port.run(self.vec, self.prepared[k])
+                dt = time.perf_counter() - t0
+                if record:
+                    self.times[c].append(dt)
+                if time.perf_counter() - t_all > budget_s:
+                    return time.perf_counter() - t_all
+        return time.perf_counter() - t_all
+
+    def estimate(self):
+        """(gates/s, {class: mean s/gate}, gates timed) from the samples so far."""
+        per = {c: sum(t) / len(t) for c, t in self.times.items() if t}
+        if len(per) < len(self.classes):
+            missing = [c for c in self.classes if c not in per]
+            raise RuntimeError(f"no timing sample for gate classes {missing}")
+        total_s = sum(len(self.classes[c]) * per[c] for c in self.classes)
+        return self.total / total_s, per, sum(len(t) for t in self.times.values())
+
+    def describe(self, gates_timed, seconds):
+        counts = {c: len(i) for c, i in self.classes.items()}
+        return (f"{gates_timed} gates of the 1000-gate {self.n}q c128 config-1 circuit timed in {seconds:.1f} s, "
+                f"stratified by gate class {counts}; rate = 1000 / sum(count x mean s/gate) "
+                f"(numba restatement of QuICT cpu_calculator kernels)")
 
     @staticmethod
     def threads():
@@ -187,32 +223,47 @@ class CpuBaseline:
         return numba.get_num_threads()
 
 
+def one_thread_baseline(circuit_fn, n_small=26, n=30):
+    """The port on ONE host thread (the reference's own numba kernels are
+    single-threaded) at n_small qubits, one gate per class, scaled by
+    2^(n - n_small) to n qubits (time per gate is linear in the amplitudes)."""
+    cb = CpuBaseline(circuit_fn(n_small), n_small, threads=1)
+    secs = cb.sample(rounds=1)
+    r, per, k = cb.estimate()
+    scale = 2.0 ** (n - n_small)
+    import numba
+    numba.set_num_threads(numba.config.NUMBA_NUM_THREADS)
+    return {"value": r / scale, "unit": "gates/s", "cores": 1, "kind": "port",
+            "s_per_gate_by_class": {c: v * scale for c, v in per.items()},
+            "sample": f"one gate per class at {n_small} qubits on 1 thread ({secs:.1f} s), "
+                      f"scaled by 2^{n - n_small} to {n} qubits (extrapolated)"}
+
+
 def run_reference(args, ws, rank):
-    """--impl reference: the reference CPU algorithm (numba port) on the same workload."""
+    """--impl reference: the reference CPU algorithm (numba port, every host
+    thread) on the same workload; each step times one gate of every class."""
     if rank != 0:
         return
     from quict_b200.workloads import config1_circuit
     circuit = config1_circuit(N_QUBITS, N_GATES, SEED)
     cb = CpuBaseline(circuit, N_QUBITS)
-    per_step = max(1, args.ref_gates // max(1, args.steps))
-    pos, rates = 0, []
-    for s in range(args.warmup + args.steps):
-        r, done, dt = cb.step(pos, args.ref_budget / max(1, args.steps), 1 if s < args.warmup else per_step)
-        pos += done
-        if s >= args.warmup:
-            rates.append(r)
-    v = statistics.median(rates)
+    for _ in range(args.warmup):
+        cb.sample(rounds=1, record=False)
+    secs = cb.sample(rounds=args.steps)
+    v, per, timed = cb.estimate()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "gates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded config-1 circuit)",
         "config": {"workload": f"sv-{N_QUBITS}q-c128-{N_GATES}g-config1", "qubits": N_QUBITS,
-                   "gates_per_step": per_step, "seed": SEED},
+                   "gates_per_step": len(cb.classes), "seed": SEED},
         "cpu_baseline": {"value": v, "unit": "gates/s", "cores": cb.threads(), "kind": "port",
-                         "sample": f"{per_step} gates of the 1000-gate 30q c128 circuit per step "
-                                   f"(numba restatement of QuICT cpu_calculator kernels, all host threads)"},
+                         "s_per_gate_by_class": per, "sample": cb.describe(timed, secs)},
         "e2e": {"value": v, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.ref_one_thread:
+        line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: config1_circuit(q, N_GATES, SEED),
+                                                           n=N_QUBITS)
     print(json.dumps(line), flush=True)
 
 
@@ -617,10 +668,13 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         torch.cuda.empty_cache()
         cb = CpuBaseline(circuit, n)
-        r, done, dt = cb.step(0, args.ref_budget, args.ref_gates)
+        cb.sample(rounds=1, record=False)  # first touch of the host state
+        secs = cb.sample(rounds=args.ref_rounds, budget_s=args.ref_budget)
+        r, per, timed = cb.estimate()
         line["cpu_baseline"] = {"value": r, "unit": "gates/s", "cores": cb.threads(), "kind": "port",
-                                "sample": f"first {done} gates of the same 30q c128 circuit "
-                                          f"({dt:.1f} s, numba restatement of QuICT cpu_calculator kernels)"}
+                                "s_per_gate_by_class": per, "sample": cb.describe(timed, secs)}
+        if args.ref_one_thread:
+            line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: config1_circuit(q, N_GATES, SEED), n=n)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -632,8 +686,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
-    ap.add_argument("--ref-gates", type=int, default=24)
-    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--ref-rounds", type=int, default=2,
+                    help="CPU baseline: gates timed per gate class (one per round)")
+    ap.add_argument("--ref-budget", type=float, default=40.0, help="CPU baseline: seconds at most")
+    ap.add_argument("--ref-one-thread", type=int, default=1,
+                    help="also time the port on one thread (26 qubits, scaled to 30)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
     ap.add_argument("--tile-bits", type=int, default=None, help="fused tile width k (default: the tuning cache)")

@@ -70,7 +70,9 @@ extern "C" {
 /* ---- probability sources and sampling modes ------------------------------ */
 #define QS_SRC_SV  0      /* p_i = |vec[i]|^2                                  */
 #define QS_SRC_DM  1      /* p_i = Re rho[i, i] of a 2^n x 2^n density matrix  */
-#define QS_SAMPLE_CDF  0  /* one uniform per shot: smallest i with u <= CDF[i] */
+#define QS_SAMPLE_CDF  0  /* one uniform per shot: smallest i with
+                             u * total <= CDF[i] (FP64, unnormalised CDF);
+                             indices of probability 0 are never returned    */
 #define QS_SAMPLE_SEQ  1  /* n uniforms per shot, qubit 0 (MSB) first, outcome
                              1 iff u > P(0) -- the reference's per-qubit rule  */
 
@@ -239,9 +241,11 @@ int qs_sample(const void* src, int n, int dtype, int src_kind, const void* ws,
  * device array of the library (1 MiB on every device that loads it, held until
  * the process exits), so the call allocates nothing and frees nothing.
  * Limit: n <= QS_NOALLOC_SAMPLE_MAX_QUBITS (26); larger n returns QS_EINVAL.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture begins.  All calls share the one array and it
+ * Each call made outside stream capture looks up the array's device address
+ * on the current device (cudaGetSymbolAddress, with that device current), so
+ * a context rebuilt by cudaDeviceReset is handled; a call inside a capture
+ * reuses the address the last call outside one found, so make the first
+ * call on each device before any stream capture begins.  All calls share the one array and it
  * keeps the last call's contents (each call overwrites every node it reads),
  * so calls whose work overlaps on the GPU -- e.g. on two streams -- race:
  * order them on one stream.  Arguments and results as qs_sample. */

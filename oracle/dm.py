@@ -95,17 +95,36 @@ def apply_channel(rho: np.ndarray, n: int, ks: Sequence[np.ndarray], args: Seque
     return out.reshape(1 << n, 1 << n)
 
 
+def apply_superop(rho: np.ndarray, n: int, ks: Sequence[np.ndarray], args: Sequence[int]) -> np.ndarray:
+    """The same map as ``apply_channel`` in one contraction: the channel's
+    superoperator S = sum_i K_i (x) conj(K_i) (rows (r_out, c_out), columns
+    (r_in, c_in), each big-endian over `args`) times rho's (row bits of args,
+    column bits of args) axes, as one matrix product.  Equal to the Kraus sum
+    up to FP64 rounding; fast enough for 12-qubit, 150-gate runs."""
+    k = len(args)
+    S = sum(np.kron(np.asarray(K, dtype=np.complex128), np.conj(np.asarray(K, dtype=np.complex128))) for K in ks)
+    axes = list(args) + [n + a for a in args]
+    t = np.moveaxis(rho.reshape([2] * (2 * n)), axes, list(range(2 * k)))
+    front = t.shape
+    y = (S @ t.reshape(1 << (2 * k), -1)).reshape(front)
+    return np.ascontiguousarray(np.moveaxis(y, list(range(2 * k)), axes)).reshape(1 << n, 1 << n)
+
+
 def run(gates, n: int, rho: Optional[np.ndarray] = None,
-        noise: Optional[Callable[[Sequence[int]], Optional[List[np.ndarray]]]] = None) -> np.ndarray:
+        noise: Optional[Callable[[Sequence[int]], Optional[List[np.ndarray]]]] = None,
+        superop: bool = False) -> np.ndarray:
     """Apply [(U, args)]; when noise(args) returns Kraus ops K_i, the gate is
-    replaced by the channel {K_i U} (accumulated mode)."""
+    replaced by the channel {K_i U} (accumulated mode).  `superop` applies each
+    channel as one superoperator product (``apply_superop``) instead of a
+    Kraus sum."""
+    apply = apply_superop if superop else apply_channel
     r = zero_dm(n) if rho is None else np.asarray(rho, dtype=np.complex128).copy()
     for U, args in gates:
         ks = noise(args) if noise is not None else None
         if ks:
-            r = apply_channel(r, n, [K @ U for K in ks], args)
+            r = apply(r, n, [K @ U for K in ks], args)
         else:
-            r = apply_channel(r, n, [U], args)
+            r = apply(r, n, [U], args)
     return r
 
 

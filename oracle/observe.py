@@ -17,8 +17,34 @@ from . import sv as osv
 
 
 def energy(gates, n, hmat):
+    """<psi|H|psi>; `hmat` a dense matrix, or a Pauli sum as a list of
+    (coefficient, {qubit: 'X'|'Y'|'Z'}) terms (see ``pauli_expect``)."""
     psi = osv.run(gates, n)
+    if isinstance(hmat, list):
+        return pauli_expect(psi, n, hmat)
     return float(np.real(np.vdot(psi, hmat @ psi)))
+
+
+def pauli_expect(psi, n, terms):
+    """sum_t c_t <psi|P_t|psi> without a dense H: a Pauli string with X-part
+    mask x and Z-part mask z (vector bits; qubit q is bit n-1-q, Y = i X Z)
+    maps amplitude j to (i^|x & z|) (-1)^|z & j| at index j ^ x."""
+    idx = np.arange(1 << n, dtype=np.int64)
+    total = 0.0
+    for c, ps in terms:
+        x = z = 0
+        for q, p in ps.items():
+            b = 1 << (n - 1 - q)
+            if p in ("X", "Y"):
+                x |= b
+            if p in ("Z", "Y"):
+                z |= b
+        src = idx ^ x
+        par = np.bitwise_count(src & z) & 1
+        phase = (1j) ** bin(x & z).count("1")
+        p_psi = phase * (1.0 - 2.0 * par) * psi[src]
+        total += float(np.real(complex(c) * np.vdot(psi, p_psi)))
+    return total
 
 
 def param_shift(matrices_fn, params, n, hmat, occurrences):
@@ -40,3 +66,27 @@ def finite_diff(matrices_fn, params, n, hmat, h=1e-5):
         p2[k] -= h
         g[k] = (energy(matrices_fn(p1, {}), n, hmat) - energy(matrices_fn(p2, {}), n, hmat)) / (2 * h)
     return g
+
+
+def shift_energies(base, n, hmat, shifted):
+    """Energies of the circuit `base` ([(matrix, qubits)]) with one gate
+    replaced at a time: `shifted` = [(entry, m_plus, m_minus)] in ascending
+    entry order gives [(E with gate entry = m_plus, E with m_minus)].  The state
+    before each entry is carried forward once, so the cost per entry is two
+    runs of the gates after it."""
+    out = []
+    psi = osv.zero_state(n)
+    at = 0
+    for entry, mp, mm in shifted:
+        for m, q in base[at:entry]:
+            psi = osv.apply_matrix(psi, n, m, q)
+        at = entry
+        pair = []
+        for m in (mp, mm):
+            v = osv.apply_matrix(psi, n, m, base[entry][1])
+            for m2, q2 in base[entry + 1:]:
+                v = osv.apply_matrix(v, n, m2, q2)
+            pair.append(pauli_expect(v, n, hmat) if isinstance(hmat, list)
+                        else float(np.real(np.vdot(v, hmat @ v))))
+        out.append(tuple(pair))
+    return out

@@ -28,6 +28,14 @@ def zero_state(n: int) -> np.ndarray:
 def apply_matrix(vec: np.ndarray, n: int, mat: np.ndarray, args: Sequence[int]) -> np.ndarray:
     """vec <- (mat on circuit qubits `args`, big-endian) vec.  Returns a new array."""
     k = len(args)
+    if k == 1:  # the common case, as two strided row updates (qubit q = axis q)
+        q = args[0]
+        m = np.asarray(mat, dtype=np.complex128)
+        v3 = np.asarray(vec, dtype=np.complex128).reshape(1 << q, 2, -1)
+        out = np.empty_like(v3)
+        out[:, 0, :] = m[0, 0] * v3[:, 0, :] + m[0, 1] * v3[:, 1, :]
+        out[:, 1, :] = m[1, 0] * v3[:, 0, :] + m[1, 1] * v3[:, 1, :]
+        return out.reshape(-1)
     t = np.asarray(mat, dtype=np.complex128).reshape([2] * (2 * k))
     psi = vec.reshape([2] * n)
     out = np.tensordot(t, psi, axes=(list(range(k, 2 * k)), list(args)))
@@ -127,20 +135,33 @@ def sample_sequential_fast(vec: np.ndarray, n: int, uniforms: np.ndarray) -> np.
 
 
 def sample_cdf(vec: np.ndarray, uniforms: np.ndarray) -> np.ndarray:
-    """One uniform per shot: smallest i with u <= CDF[i] (FP64 cumulative sum).
+    """One uniform per shot: smallest i with u * total <= CDF[i] (FP64
+    cumulative sum, total = CDF[-1]), never an index of probability 0.
     By the chain rule this is the reference's sequential rule fed the derived
-    uniform stream u_{k+1} = u_k / p0 or (u_k - p0) / (1 - p0)."""
+    uniform stream u_{k+1} = u_k / p0 or (u_k - p0) / (1 - p0); scaling u by
+    the total makes it a distribution over the state's own mass when its norm
+    has drifted from 1 (complex64 rounding, a density matrix's trace)."""
     p = np.abs(np.asarray(vec)) ** 2
+    return _cdf_pick(p, uniforms)
+
+
+def _cdf_pick(p: np.ndarray, uniforms: np.ndarray) -> np.ndarray:
     cdf = np.cumsum(p)
-    idx = np.searchsorted(cdf, np.asarray(uniforms, dtype=np.float64), side="left")
-    return np.minimum(idx, p.size - 1).astype(np.int64)
+    nz = np.flatnonzero(p > 0)
+    if nz.size == 0:
+        return np.zeros(np.asarray(uniforms).shape, dtype=np.int64)
+    t = np.asarray(uniforms, dtype=np.float64) * cdf[-1]
+    idx = np.searchsorted(cdf, t, side="left")
+    # a flat CDF run (p = 0) is never the first index reaching t, except
+    # before the first nonzero probability (t = 0) and past the end (rounding)
+    return np.clip(idx, nz[0], nz[-1]).astype(np.int64)
 
 
 def near_ties(vec: np.ndarray, uniforms: np.ndarray, tol: float = 1e-12) -> np.ndarray:
     """Mask of uniforms within `tol` of a CDF boundary (where FP64 summation
     order may legitimately change the sampled index)."""
     cdf = np.cumsum(np.abs(np.asarray(vec)) ** 2)
-    u = np.asarray(uniforms, dtype=np.float64)
+    u = np.asarray(uniforms, dtype=np.float64) * cdf[-1]
     j = np.searchsorted(cdf, u)
     d = np.full(u.shape, np.inf)
     for off in (-1, 0):

@@ -27,6 +27,7 @@ QS_SRC_SV, QS_SRC_DM = 0, 1
 QS_SAMPLE_CDF, QS_SAMPLE_SEQ = 0, 1
 QS_MAX_TILE_BITS = 14
 QS_MAX_PASS_OPS = 160
+QS_NOALLOC_SAMPLE_MAX_QUBITS = 26
 
 
 class NativeLibraryError(RuntimeError):

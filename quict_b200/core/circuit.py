@@ -5,6 +5,9 @@
 - ``Qureg`` converts to an int big-endian: qubit 0 is the most significant
   bit (QuICT/core/qubit/qubit.py:192-213).
 - ``get_lastcall_for_each_qubits`` (QuICT/core/utils/circuit_info.py:153-167).
+- CheckPoints and composite gates: ``cp | circuit`` marks the current end,
+  ``cgate | circuit`` inserts at the mark of the composite gate's checkpoint
+  child, and ``find_position`` moves the marks (circuit.py:297-360).
 """
 from __future__ import annotations
 
@@ -47,6 +50,7 @@ class Circuit:
         self.name = name
         self._qubits = Qureg(Qubit() for _ in range(wires))
         self._gates: List = []
+        self._checkpoints: List = []
         self._pointer: Optional[List[int]] = None
         self._precision = np.complex128 if precision == "double" else np.complex64
 
@@ -76,22 +80,69 @@ class Circuit:
     def __getitem__(self, item):
         return self._qubits[item]
 
-    def append(self, op):
+    def append(self, op, insert_idx: int = -1):
+        from .operator import CheckPoint
         args = self._pointer
         self._pointer = None
         if isinstance(op, BasicGate):
-            self._add_gate(op, args)
+            self._add_gate(op, args, insert_idx)
+        elif isinstance(op, CheckPoint):
+            # a mark at the current end (check_point.py:44-47); not a gate
+            op._pos = self.size()
+            self._checkpoints.append(op)
         else:
             # operators (NoiseGate, Trigger-like): keep as given
             if args is not None and hasattr(op, "targs"):
+                if len(args) != getattr(op, "targets", len(args)):
+                    raise ValueError(f"operator acts on {op.targets} qubits, got {len(args)}")
                 op.targs = list(args)
-            self._gates.append(op)
+            if insert_idx < 0:
+                self._gates.append(op)
+            else:
+                self._gates.insert(insert_idx, op)
 
     def extend(self, gates):
+        """Append `gates` (a list or a CompositeGate).  A composite gate with
+        a checkpoint child goes in at its checkpoint's mark (circuit.py:340-360);
+        ``circuit(qubits)`` before it maps the composite gate's qubit i to
+        qubits[i]."""
+        from .operator import CompositeGate
+        mapping = self._pointer
+        self._pointer = None
+        position = -1
+        if isinstance(gates, CompositeGate):
+            position = self.find_position(gates.checkpoint)
+            gates = gates.gates
         for g in gates:
-            self._gates.append(g.copy() if isinstance(g, BasicGate) else g)
+            if isinstance(g, BasicGate):
+                g = g.copy()
+                if mapping is not None:
+                    g.cargs = [mapping[q] for q in g.cargs]
+                    g.targs = [mapping[q] for q in g.targs]
+                self._add_gate(g, None, position)
+            elif position < 0:
+                self._gates.append(g)
+            else:
+                self._gates.insert(position, g)
+            if position >= 0:
+                position += 1
 
-    def _add_gate(self, gate: BasicGate, args: Optional[List[int]]):
+    def find_position(self, cp_child) -> int:
+        """Mark of the checkpoint `cp_child` belongs to (-1 for None); that
+        mark and every later one then move by the child's shift
+        (circuit.py:297-310)."""
+        position = -1
+        if cp_child is None:
+            return position
+        for cp in self._checkpoints:
+            if cp.uid == cp_child.uid:
+                position = cp.position
+                cp.position = cp_child.shift
+            elif position != -1:
+                cp.position = cp_child.shift
+        return position
+
+    def _add_gate(self, gate: BasicGate, args: Optional[List[int]], insert_idx: int = -1):
         size = gate.controls + gate.targets
         if args is None:
             assigned = gate.cargs + gate.targs
@@ -99,7 +150,9 @@ class Circuit:
                 args = assigned
             elif size == 1:
                 for q in range(self.width()):
-                    self._add_gate(gate, [q])
+                    self._add_gate(gate, [q], insert_idx)
+                    if insert_idx >= 0:
+                        insert_idx += 1
                 return
             elif size == self.width():
                 args = list(range(self.width()))
@@ -114,7 +167,10 @@ class Circuit:
         g.targs = list(args[gate.controls:])
         if g.precision != self._precision:
             g.convert_precision()
-        self._gates.append(g)
+        if insert_idx < 0:
+            self._gates.append(g)
+        else:
+            self._gates.insert(insert_idx, g)
 
     def get_lastcall_for_each_qubits(self) -> List[Optional[GateType]]:
         last: List[Optional[GateType]] = [None] * self.width()

@@ -407,6 +407,34 @@ class PermGate(BasicGate):
         return g
 
 
+class PermFxGate(BasicGate):
+    """Oracle of a boolean function f on n qubits, acting on n + 1:
+    |x, y> -> |x, y XOR f(x)>, f(x) = 1 for x in `params`; y is the last
+    target (the least significant bit of the big-endian index).  pargs[i]
+    is the column of the 1 in row i (gate.py:2176-2229)."""
+
+    def __init__(self, targets: int = 0):
+        super().__init__(GateType.perm_fx, 0, targets, 0, MatrixType.normal)
+
+    def __call__(self, n: int, params: list) -> "PermFxGate":
+        if not isinstance(params, list) or not isinstance(n, int):
+            raise TypeError(f"n must be int ({type(n)}) and params a list ({type(params)})")
+        if any(not 0 <= p < (1 << n) for p in params):
+            raise ValueError("PermFx params must lie in [0, 2^n)")
+        ones = set(int(p) for p in params)
+        g = PermFxGate(n + 1)
+        g._params = 1 << (n + 1)
+        g._pargs = [idx ^ 1 if (idx >> 1) in ones else idx for idx in range(1 << (n + 1))]
+        return g
+
+    @property
+    def matrix(self) -> np.ndarray:
+        d = 1 << self._targets
+        m = np.zeros((d, d), dtype=self._precision)
+        m[np.arange(d), np.asarray(self._pargs, dtype=np.int64)] = 1
+        return m
+
+
 def _make(t: GateType) -> BasicGate:
     c, tg, p, mt, fn = _SPEC[t]
     if p == 0 and fn is not None:  # a fixed gate: its matrix is built once
@@ -462,9 +490,10 @@ Unitary = UnitaryGate()
 QFT = QFTGate()
 IQFT = QFTGate(inverse=True)
 Perm = PermGate()
+PermFx = PermFxGate()
 
 # QASM / generator name -> gate template
 GATE_BY_NAME = {
     t.name: _make(t) for t in _SPEC
 }
-GATE_BY_NAME.update({"unitary": Unitary, "qft": QFT, "iqft": IQFT, "perm": Perm})
+GATE_BY_NAME.update({"unitary": Unitary, "qft": QFT, "iqft": IQFT, "perm": Perm, "perm_fx": PermFx})

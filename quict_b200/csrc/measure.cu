@@ -126,6 +126,17 @@ __global__ void __launch_bounds__(kThreads) k_level(double* __restrict__ tree, u
     }
 }
 
+// CDF descent step: go right when u lies beyond the left half's mass, but
+// never into a half of zero mass.  The in-block half sums are added in a
+// different order from the leaf sums above them, so u can exceed a block's
+// recomputed total by a rounding error; the guard then ends the descent on
+// the block's last element of nonzero probability instead of one with p = 0.
+__device__ __forceinline__ bool cdf_right(double uc, double acc, double sl, double sr) {
+    if (!(sr > 0.0)) return false;
+    if (!(sl > 0.0)) return true;
+    return !(uc <= acc + sl);
+}
+
 // One warp per shot.  Within the leaf block lane l owns elements
 // [l*E, (l+1)*E), E = 2^bb / 32 (or one element per lane for tiny blocks).
 template <typename V, int SRC, int MODE>
@@ -140,7 +151,11 @@ k_sample(const V* __restrict__ s, int n, uint64_t nleaf, int bb, uint64_t dstrid
     const int E = bsz >= 32 ? bsz / 32 : 1;
     for (int64_t shot = int64_t(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5); shot < shots; shot += warps) {
         const double* us = MODE == QS_SAMPLE_SEQ ? u + shot * n : u + shot;
-        double uc = us[0];
+        // CDF mode compares against unnormalised FP64 partial sums, so the
+        // uniform is scaled by the total mass (the root): a state whose norm
+        // has drifted below 1 (complex64, a density matrix's trace) then
+        // never runs off the end of the distribution
+        double uc = MODE == QS_SAMPLE_SEQ ? us[0] : us[0] * tree[1];
         double acc = 0.0;  // CDF mode: mass strictly left of the current node
         uint64_t node = 1;
         for (int lvl = 0; lvl < top; ++lvl) {
@@ -151,7 +166,7 @@ k_sample(const V* __restrict__ s, int n, uint64_t nleaf, int bb, uint64_t dstrid
                 right = uc > sl / tot;
                 uc = us[lvl + 1 < n ? lvl + 1 : n - 1];
             } else {
-                right = !(uc <= acc + sl);
+                right = cdf_right(uc, acc, sl, sr);
                 if (right) acc += sl;
             }
             node = 2 * node + (right ? 1 : 0);
@@ -195,7 +210,7 @@ k_sample(const V* __restrict__ s, int n, uint64_t nleaf, int bb, uint64_t dstrid
                 right = uc > sl / (sl + sr);
                 uc = us[lvl + 1 < n ? lvl + 1 : n - 1];
             } else {
-                right = !(uc <= acc + sl);
+                right = cdf_right(uc, acc, sl, sr);
                 if (right) acc += sl;
             }
             if (right) lo += half;
@@ -397,9 +412,12 @@ constexpr size_t kNoAllocTreeDoubles = size_t(2) << (kNoAllocMaxQubits - kBlockB
 static __device__ __align__(256) double g_noalloc_tree[kNoAllocTreeDoubles];
 
 namespace {
-// Device address of g_noalloc_tree, looked up once per device with that device
-// current (the array's host-side name is not a device address).
-int noalloc_tree_ptr(double** out) {
+// Device address of g_noalloc_tree on the current device (the array's
+// host-side name is not a device address).  It is looked up with that device
+// current on every call made outside stream capture, so a context rebuilt
+// after cudaDeviceReset gets its new address; inside a capture the address
+// recorded by the last call outside one is used.
+int noalloc_tree_ptr(cudaStream_t st, double** out) {
     static std::mutex mu;
     static double* addr[64] = {nullptr};
     int dev = 0;
@@ -409,8 +427,14 @@ int noalloc_tree_ptr(double** out) {
         return QS_ECUDA;
     }
     QS_REQUIRE(dev >= 0 && dev < 64, "qs_sample_noalloc: device %d outside [0, 64)", dev);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) {
+        set_error("qs_sample_noalloc: cudaStreamIsCapturing: %s", cudaGetErrorString(e));
+        return QS_ECUDA;
+    }
     std::lock_guard<std::mutex> lock(mu);
-    if (addr[dev] == nullptr) {
+    if (addr[dev] == nullptr || cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_tree);
         if (e != cudaSuccess || p == nullptr) {
@@ -438,12 +462,12 @@ extern "C" int qs_sample_noalloc(const void* src, int n, int dtype, int src_kind
     QS_REQUIRE(shots >= 0, "negative shot count");
     QS_REQUIRE(u_dev != nullptr && out_idx_dev != nullptr, "null uniforms or output");
     if (shots == 0) return QS_OK;
+    cudaStream_t st = as_stream(stream);
     double* tree = nullptr;
-    rc = noalloc_tree_ptr(&tree);
+    rc = noalloc_tree_ptr(st, &tree);
     if (rc) return rc;
     // every node the descent reads is written by the prepare step, so the
     // tree needs no clearing between calls
-    cudaStream_t st = as_stream(stream);
     if (dtype == QS_C128) {
         rc = prepare_t<double2>(src, n, src_kind, tree, st);
         return rc ? rc : sample_t<double2>(src, n, src_kind, tree, u_dev, shots, mode, out_idx_dev, st);

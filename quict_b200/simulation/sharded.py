@@ -356,12 +356,14 @@ class ShardedStateVector:
 
     def sample(self, shots: int, uniforms=None, seed: Optional[int] = None) -> np.ndarray:
         """Basis indices of `shots` samples, one uniform per shot, on every
-        rank: the smallest global index i with u <= CDF[i] (FP64), the rule of
-        ``StateVectorSimulator.sample(mode="cdf")``.  The shot's rank comes
-        from the cumulative shard masses; that rank then finds the index in its
-        own shard for u minus the mass of the ranks before it.  `uniforms`, if
-        given, must be the same on every rank; otherwise rank 0 draws them
-        (numpy ``default_rng(seed)``) and broadcasts them."""
+        rank: the smallest global index i with u * total <= CDF[i] (FP64),
+        the rule of ``StateVectorSimulator.sample(mode="cdf")``.  The shot's
+        rank comes from the cumulative shard masses (never a rank of zero
+        mass); that rank then samples its own shard with the uniform
+        (u * total - mass of the ranks before it) / its own mass, which its
+        sampler scales back by that mass.  `uniforms`, if given, must be the
+        same on every rank; otherwise rank 0 draws them (numpy
+        ``default_rng(seed)``) and broadcasts them."""
         self.canonical()
         dev = self._reduce_dev()
         if uniforms is None:
@@ -378,13 +380,17 @@ class ShardedStateVector:
             parts = [torch.empty_like(mass) for _ in range(self.world)]
             dist.all_gather(parts, mass, group=self.group)
             mass = torch.cat(parts)
-        cdf = np.cumsum(mass.cpu().numpy())
-        owner = np.minimum(np.searchsorted(cdf, u, side="left"), self.world - 1)
+        m = mass.cpu().numpy()
+        cdf = np.cumsum(m)
+        live = np.flatnonzero(m > 0)
+        t = u * cdf[-1]
+        owner = np.searchsorted(cdf, t, side="left")
+        owner = np.clip(owner, live[0], live[-1]) if live.size else np.zeros_like(owner)
         mine = np.flatnonzero(owner == self.rank)
         out = np.zeros(shots, dtype=np.int64)
         if mine.size:
             before = cdf[self.rank - 1] if self.rank > 0 else 0.0
-            ul = torch.as_tensor(u[mine] - before, dtype=torch.float64)
+            ul = torch.as_tensor(np.clip((t[mine] - before) / m[self.rank], 0.0, 1.0), dtype=torch.float64)
             idx = self.backend.sample_indices(self.local, self.nl, ul, N.QS_SAMPLE_CDF)
             out[mine] = (np.asarray(idx.cpu().numpy() if hasattr(idx, "cpu") else idx, dtype=np.int64)
                          + (self.rank << self.nl))

@@ -174,9 +174,9 @@ class StateVectorSimulator:
             if _is_trigger(g):
                 self._engine.apply_ops(self._vector, n, pending)
                 pending = []
-                extra = self.apply_trigger(g)
+                extra, position = self.apply_trigger(g, idx)
                 if extra:
-                    gates[idx:idx] = list(extra)
+                    gates[position:position] = list(extra)
                 continue
             for op in lower_gate(g, n, self._legacy):
                 if op.kind in ("measure", "reset", "perm"):
@@ -243,8 +243,14 @@ class StateVectorSimulator:
         self._vector = torch.zeros_like(self._vector)
 
     def apply_trigger(self, op, current_idx: int = 0):
-        """Measure the trigger's qubits, then return the gates its mapping selects
-        (statevector_simulator.py:498-523)."""
+        """Measure the trigger's qubits, then return (gates, position): the
+        gates its mapping selects for the measured value and the index of
+        the run's gate list where they go in (statevector_simulator.py:498-523).
+        That is `current_idx` (the index after the trigger), or, when the
+        selected composite gate carries a checkpoint child, the mark of its
+        CheckPoint in the circuit (``Circuit.find_position``, which also moves
+        the marks by the child's shift).  A plain gate or None selects that
+        gate alone or nothing."""
         n = self._qubits
         for q in op.targs:
             self._measure_bit(n - 1 - q)
@@ -252,7 +258,13 @@ class StateVectorSimulator:
         for q in op.targs:
             value = (value << 1) | int(self._circuit.qubits[q].measured)
         cg = op.mapping(value)
-        return list(cg.gates) if cg is not None else []
+        if cg is None:
+            return [], current_idx
+        if not hasattr(cg, "gates"):  # a single gate
+            return [cg], current_idx
+        cp = getattr(cg, "checkpoint", None)
+        position = current_idx if cp is None else self._circuit.find_position(cp)
+        return list(cg.gates), position
 
     # ---- sampling ---------------------------------------------------------------------------
     def sample(self, shots: int = 1, uniforms=None, mode: str = "cdf", seed: Optional[int] = None,

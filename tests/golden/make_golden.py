@@ -1,14 +1,14 @@
 """Generate the golden fixtures in tests/golden/ by running the REFERENCE
 (taofei95/quict) CPU simulators in this container.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <QuICT checkout> [--only core,dynamic,dropin]
 
 The reference is imported with stub modules for its plotting / QASM-lexer
 dependencies (matplotlib, IPython, ply, pylatexenc, prettytable), which are
 off the arithmetic path, and with numpy.complex restored (removed in numpy 2,
 used in an annotation at statevector_simulator.py:525).  Only derived data is
 written: gate lists, amplitudes, density matrices, counts and the uniforms the
-reference consumed.  Nothing under /root/reference is copied.
+reference consumed.  Nothing of the reference checkout is copied.
 
 Fixtures
   gates.json          matrix / matrix_type / arity of every reference gate type
@@ -23,6 +23,11 @@ Fixtures
   sample.npz          reference CPU sample() counts with the numba-RNG uniforms
   midmeasure.npz      Measure / Reset inside a circuit with recorded uniforms
   dm.npz              reference DensityMatrixSimulator with noise (n=3, 4)
+  grad.npz            energies and parameter-shift gradients (HEA, QAOA)
+  dynamic.npz         PermFx oracles, QFT / IQFT, Triggers with and without
+                      CheckPoints with the numba-RNG uniforms they consumed
+  dropin.npz          real QuICT.core circuits as lowered by quict_b200 (the
+                      ops its simulators run), with gate lists to rebuild them
 """
 from __future__ import annotations
 
@@ -128,11 +133,8 @@ def haar(rng, d):
     return q * (np.diag(r) / np.abs(np.diag(r)))
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    a = ap.parse_args()
-    shim(a.ref)
+def core_fixtures(ref: str):
+    """gates.json ... grad.npz (see the module docstring)."""
     from QuICT.core.gate import GATE_TYPE_TO_CLASS, GateType
 
     # ---- gate matrices ---------------------------------------------------------------
@@ -149,9 +151,9 @@ def main():
     json.dump(gates, open(os.path.join(HERE, "gates.json"), "w"))
 
     # ---- the reference's own golden circuit ---------------------------------------------
-    qasm = os.path.join(a.ref, "unit_test/simulation/data/random_circuit_for_correction.qasm")
+    qasm = os.path.join(ref, "unit_test/simulation/data/random_circuit_for_correction.qasm")
     n, gl = parse_qasm(qasm)
-    golden = np.load(os.path.join(a.ref, "unit_test/simulation/data/state_vector.npy"))
+    golden = np.load(os.path.join(ref, "unit_test/simulation/data/state_vector.npy"))
     ours = sv_cpu(build(gl, n))
     assert np.allclose(ours, golden, atol=1e-12), "reference CPU SV does not reproduce its golden vector"
     json.dump({"n": n, "gates": gl}, open(os.path.join(HERE, "qasm_circuit.json"), "w"))
@@ -354,6 +356,196 @@ def main():
     out["qaoa_edges"], out["qaoa_params"] = np.array(edges), gb
     out["qaoa_energy"], out["qaoa_grad"] = energy(qaoa_gates(gb), n, cost), gq
     np.savez_compressed(os.path.join(HERE, "grad.npz"), **out)
+
+
+def dynamic_fixtures(ref: str):
+    """dynamic.npz: PermFx oracles, QFT / IQFT and Triggers with and without CheckPoints,
+    run by the reference CPU StateVectorSimulator; the measurement uniforms
+    come from the reference's numba RNG, seeded before each run, and are
+    recorded."""
+    import numba
+    import random
+    from QuICT.core import Circuit
+    from QuICT.core.gate import CompositeGate, CX, H, PermFx, Rx, Ry, Rz, X, Y, Swap
+    from QuICT.core.operator import CheckPoint, Trigger
+    from QuICT.simulation.state_vector import StateVectorSimulator
+
+    @numba.njit
+    def nb_seed(s):
+        random.seed(s)
+
+    @numba.njit
+    def nb_draw(k):
+        r = np.empty(k)
+        for i in range(k):
+            r[i] = random.random()
+        return r
+
+    out = {}
+    # ---- PermFx: |x, y> -> |x, y ^ f(x)> on n + 1 qubits, behind H layers
+    rng = np.random.default_rng(601)
+    for n in (1, 2, 3, 4):
+        width = n + 2
+        ones = sorted(int(x) for x in rng.choice(1 << n, max(1, (1 << n) // 2), replace=False))
+        args = [int(x) for x in rng.permutation(width)[: n + 1]]
+        c = Circuit(width)
+        for q in range(width):
+            H | c(q)
+            Ry(float(rng.uniform(0, 2 * np.pi))) | c(q)
+        PermFx(n, ones) | c(args)
+        Rz(0.4) | c(0)
+        out[f"permfx{n}_ones"] = np.array(ones)
+        out[f"permfx{n}_args"] = np.array(args)
+        out[f"permfx{n}_width"] = np.array(width)
+        out[f"permfx{n}_pre"] = np.array([float(g.pargs[0]) for g in c.gates if g.type.name == "ry"])
+        out[f"permfx{n}_pargs"] = np.array(c.gates[2 * width].pargs)
+        out[f"permfx{n}_state"] = np.asarray(StateVectorSimulator(device="CPU").run(c)).copy()
+
+    # ---- QFT / IQFT: the reference's matrices (its gate-sequence build) and
+    # SV runs with the gates on scattered qubits
+    from QuICT.core.gate import IQFT, QFT
+    for k in (2, 3, 4, 5):
+        out[f"qft{k}_matrix"] = np.asarray(QFT(k).matrix, dtype=np.complex128)
+        out[f"iqft{k}_matrix"] = np.asarray(IQFT(k).matrix, dtype=np.complex128)
+        width = k + 2
+        # qubits 0..k-1 in order: the reference's QFTGate.matrix fails for a
+        # gate placed on other qubits (circuit_matrix.py:175 looks the gate's
+        # qubits up among 0..k-1), and for a permutation of them it expresses
+        # the matrix in sorted-qubit order while the gate keeps its own order
+        args = list(range(k))
+        c = Circuit(width)
+        for q in range(width):
+            Ry(float(0.3 + 0.2 * q)) | c(q)
+        QFT(k) | c(args)
+        Rz(0.7) | c(width - 1)
+        CX | c([k - 1, width - 1])
+        IQFT(k) | c(args)
+        out[f"qft{k}_args"] = np.array(args)
+        out[f"qft{k}_state"] = np.asarray(StateVectorSimulator(device="CPU").run(c)).copy()
+
+    def run_traced(c, seed):
+        nb_seed(seed)
+        u = nb_draw(8)
+        nb_seed(seed)
+        sv = np.asarray(StateVectorSimulator(device="CPU").run(c)).copy()
+        meas = np.array([-1 if q.measured is None else int(q.measured) for q in c.qubits])
+        return u, sv, meas
+
+    # ---- Trigger without a checkpoint: the selected gates run right after it
+    # (the reference's operator_unit_test.test_trigger, plus gates after it)
+    for seed in (701, 702, 703, 704):
+        c = Circuit(4)
+        H | c(0)
+        Ry(1.1) | c(1)
+        cg0 = CompositeGate()
+        X | cg0(2)
+        cg1 = CompositeGate()
+        CX | cg1([0, 1])
+        CX | cg1([1, 2])
+        CX | cg1([2, 3])
+        Trigger(1, [cg0, cg1]) | c(0)
+        Rx(0.3) | c(3)
+        CX | c([3, 1])
+        u, sv, meas = run_traced(c, seed)
+        out[f"trig_plain_{seed}_uniforms"], out[f"trig_plain_{seed}_state"] = u, sv
+        out[f"trig_plain_{seed}_measured"] = meas
+
+    # ---- Trigger on two qubits whose composite gates carry CheckPoint
+    # children: they go in at the checkpoint's mark, after the gates between
+    # the trigger and the mark; the mark then moves by the child's shift
+    for seed in (711, 712, 713, 714, 715, 716):
+        c = Circuit(5)
+        H | c(0)
+        H | c(1)
+        Ry(0.8) | c(2)
+        cp = CheckPoint()
+        cgs = []
+        for v in range(4):
+            cg = CompositeGate()
+            if v & 1:
+                X | cg(3)
+            if v & 2:
+                Y | cg(4)
+            Ry(0.2 + 0.3 * v) | cg(2)
+            Swap | cg([2, 4])
+            cp.get_child(len(cg.gates)) | cg
+            cgs.append(cg)
+        Trigger(2, cgs) | c([0, 1])
+        Rx(0.5) | c(3)
+        CX | c([2, 3])
+        cp | c
+        Rz(0.9) | c(4)
+        CX | c([3, 4])
+        Rx(0.25) | c(2)
+        u, sv, meas = run_traced(c, seed)
+        out[f"trig_cp_{seed}_uniforms"], out[f"trig_cp_{seed}_state"] = u, sv
+        out[f"trig_cp_{seed}_measured"] = meas
+    np.savez_compressed(os.path.join(HERE, "dynamic.npz"), **out)
+
+
+def dropin_fixtures(ref: str):
+    """dropin.npz: real QuICT.core circuits lowered by quict_b200's lowering
+    (the ops the simulator would run), beside the gate lists that rebuild the
+    same circuits with quict_b200.core.  The test compares the two lowerings."""
+    from QuICT.core import Circuit
+    from QuICT.core.gate import GATE_TYPE_TO_CLASS, GateType, IQFT, PermFx, QFT, Unitary
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from quict_b200.simulation.lowering import lower_circuit
+
+    out = {}
+    rng = np.random.default_rng(801)
+    cases = {
+        "cfg0": (8, gate_list_random(rng, 8, 120, CFG0)),
+        "ext": (6, [["h", [q], []] for q in range(6)] + gate_list_random(rng, 6, 120, EXT)),
+    }
+    special = [["unitary", [int(x) for x in rng.choice(7, 3, replace=False)], haar(rng, 8).tolist()],
+               ["qft", [0, 1, 2], [3]], ["iqft", [0, 1, 2, 3], [4]],
+               ["perm_fx", [4, 1, 6], [2, [1, 2]]], ["unitary", [5, 2], haar(rng, 4).tolist()]]
+    cases["special"] = (7, [["h", [q], []] for q in range(7)] + special)
+    for name, (n, gl) in cases.items():
+        c = Circuit(n)
+        ser = []
+        for nm, args, params in gl:
+            if nm == "unitary":
+                g = Unitary(np.array(params, dtype=np.complex128))
+                ps = [[complex(x).real, complex(x).imag] for x in np.ravel(params)]
+            elif nm in ("qft", "iqft"):
+                g = (QFT if nm == "qft" else IQFT)(params[0])
+                ps = params
+            elif nm == "perm_fx":
+                g = PermFx(params[0], list(params[1]))
+                ps = params
+            else:
+                g = GATE_TYPE_TO_CLASS[GateType.__members__[nm]]()
+                if params:
+                    g = g(*params)
+                ps = params
+            g | c(list(args))
+            ser.append([nm, list(args), ps])
+        ops = lower_circuit(c.gates, n)
+        out[f"{name}_n"] = np.array(n)
+        out[f"{name}_gates"] = np.array(json.dumps(ser))
+        out[f"{name}_ops"] = np.array(json.dumps([[op.kind, list(op.tbits), list(op.cbits)] for op in ops]))
+        out[f"{name}_mats"] = np.concatenate([np.asarray(op.mat, dtype=np.complex128).ravel() for op in ops])
+    np.savez_compressed(os.path.join(HERE, "dropin.npz"), **out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", required=True, help="path of the QuICT reference checkout to run")
+    ap.add_argument("--only", default="core,dynamic,dropin",
+                    help="comma list of fixture groups to write: core (gates.json .. grad.npz), dynamic, dropin")
+    a = ap.parse_args()
+    parts = set(a.only.split(","))
+    if "dropin" in parts:
+        import torch  # noqa: F401  (before the stub modules, which torch's import would trip over)
+    shim(a.ref)
+    if "core" in parts:
+        core_fixtures(a.ref)
+    if "dynamic" in parts:
+        dynamic_fixtures(a.ref)
+    if "dropin" in parts:
+        dropin_fixtures(a.ref)
     print("golden fixtures written to", HERE)
 
 

@@ -127,7 +127,7 @@ def _tiny_circuit(n, seed, size=30):
     from quict_b200.core import Circuit, GATE_BY_NAME
     from quict_b200.core.gate import GateType
     types = [GateType[nm] for nm, g in GATE_BY_NAME.items()
-             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm")
+             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm", "perm_fx")
              and g.controls + g.targets <= n]
     c = Circuit(n)
     c.random_append(size, typelist=types, seed=seed)

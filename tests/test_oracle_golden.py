@@ -139,3 +139,29 @@ def test_dm_oracle_matches_reference(n):
     np.testing.assert_allclose(np.array(k2), d[f"n{n}_kraus2"], rtol=0, atol=1e-14)
     noisy = odm.run(oracle_gates(c), n, noise=lambda args: k1 if len(args) == 1 else k2)
     np.testing.assert_allclose(noisy, d[f"n{n}_noisy"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [5, 8, 11])
+def test_cpu_port_reproduces_reference_states(n):
+    """oracle/ref_port.py (the timed CPU baseline) against the reference CPU
+    simulator's own states."""
+    from oracle import ref_port
+    from quict_b200.simulation.lowering import lower_circuit
+    d = golden("random_sv.npz")
+    gl = json.loads(str(d[f"n{n}_gates"]))
+    v = osv.zero_state(n)
+    ref_port.run(v, ref_port.prepare(lower_circuit(build_circuit(gl, n).gates, n), np.complex128))
+    np.testing.assert_allclose(v, d[f"n{n}_double"], rtol=0, atol=1e-12)
+
+
+def test_cpu_port_on_the_benchmark_circuit_shape():
+    """The port on a 12-qubit config-1 circuit (Haar 2q unitaries, low and high
+    qubits) against the FP64 oracle, on all amplitudes."""
+    from oracle import ref_port
+    from quict_b200.simulation.lowering import lower_circuit
+    from quict_b200.workloads import config1_circuit
+    n = 12
+    c = config1_circuit(n, 300, seed=3)
+    v = osv.zero_state(n)
+    ref_port.run(v, ref_port.prepare(lower_circuit(c.gates, n), np.complex128))
+    np.testing.assert_allclose(v, osv.run(oracle_gates(c), n), rtol=0, atol=1e-12)

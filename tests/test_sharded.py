@@ -68,7 +68,7 @@ class _NumpyShard:
         v[one] = 0
 
     def sample_indices(self, vec, n, uniforms, mode):
-        # smallest i with u <= CDF[i] over this shard's unnormalised masses
+        # smallest i with u * (shard mass) <= CDF[i] over this shard's masses
         from oracle import sv as osv
         return torch.as_tensor(osv.sample_cdf(vec.numpy().astype(np.complex128), uniforms.numpy()))
 
@@ -77,7 +77,7 @@ def _circuit(n, seed, size):
     from quict_b200.core import Circuit, GATE_BY_NAME
     from quict_b200.core.gate import GateType
     types = [GateType[nm] for nm, g in GATE_BY_NAME.items()
-             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm")
+             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm", "perm_fx")
              and g.controls + g.targets <= 3]
     c = Circuit(n)
     c.random_append(size, typelist=types, seed=seed)

@@ -226,7 +226,7 @@ def test_smallest_and_empty_circuits(cuda_ok, n, precision):
     from quict_b200.core import Circuit, GATE_BY_NAME
     from quict_b200.core.gate import GateType
     types = [GateType[nm] for nm, g in GATE_BY_NAME.items()
-             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm")
+             if nm not in ("measure", "reset", "barrier", "id", "unitary", "qft", "iqft", "perm", "perm_fx")
              and g.controls + g.targets <= n]
     c = Circuit(n)
     c.random_append(40, typelist=types, seed=n)
@@ -269,3 +269,38 @@ def test_sample_counts_list_sparse_and_dense(cuda_ok):
     counts = dm.sample(10, seed=1)
     idx = dm.last_sample_indices.cpu().numpy()
     assert isinstance(counts, list) and counts == np.bincount(idx, minlength=64).tolist()
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_cdf_sampling_of_a_subnormalised_state_never_picks_zero_mass(cuda_ok, precision):
+    """A state whose norm has drifted below 1 (here scaled to 1 - 1e-4) and
+    whose last amplitudes are 0: uniforms near 1 must land on the last index
+    of nonzero probability, never past it (the CDF rule scales u by the total
+    mass), through the workspace and the allocation-free entry points."""
+    import ctypes as C
+    import torch
+    from quict_b200 import _native as N
+    n = 12
+    rng = np.random.default_rng(21)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    v[-3:] = 0  # indices 2^n-3 .. 2^n-1 have probability 0
+    v /= np.linalg.norm(v)
+    v *= np.sqrt(1 - 1e-4)
+    npdt = np.complex128 if precision == "double" else np.complex64
+    from quict_b200.core import Circuit
+    s = sim(precision)
+    s.run(Circuit(n))  # sets the width; the vector is replaced next
+    s.vector = v.astype(npdt)
+    u = np.concatenate([1 - np.logspace(-16, -3, 200), rng.random(800)])
+    s.sample(u.size, uniforms=u, mode="cdf")
+    got = s.last_sample_indices.cpu().numpy()
+    assert got.max() <= (1 << n) - 4
+    vd = v.astype(npdt).astype(np.complex128)
+    ties = osv.near_ties(vd, u, 1e-12 if precision == "double" else 1e-6)
+    assert np.all((got == osv.sample_cdf(vd, u)) | ties)
+    out = torch.empty(u.size, dtype=torch.int64, device="cuda")
+    ud = torch.from_numpy(u).cuda()
+    N.call("qs_sample_noalloc", C.c_void_p(s._vector.data_ptr()), n, s._qs_dtype, N.QS_SRC_SV,
+           C.c_void_p(ud.data_ptr()), u.size, N.QS_SAMPLE_CDF, C.c_void_p(out.data_ptr()), None)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), got)

@@ -23,21 +23,33 @@ def _state(n, seed, dtype):
     return torch.from_numpy(v.astype(dtype)).cuda()
 
 
-def _with_workspace(lib, N, vec, n, dt, u, shots, mode):
+def _density(n, seed, dtype):
+    """A random n-qubit density matrix (PSD, trace 1) as a 2^n x 2^n device array."""
     import torch
+    rng = np.random.default_rng(seed)
+    a = rng.normal(size=(1 << n, 1 << n)) + 1j * rng.normal(size=(1 << n, 1 << n))
+    rho = a @ a.conj().T
+    rho /= np.trace(rho).real
+    return torch.from_numpy(np.ascontiguousarray(rho.astype(dtype))).cuda()
+
+
+def _with_workspace(lib, N, vec, n, dt, u, shots, mode, src=None):
+    import torch
+    src = N.QS_SRC_SV if src is None else src
     wsb = lib.qs_sample_ws_bytes(n)
     ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
     out = torch.empty(shots, dtype=torch.int64, device="cuda")
-    N.call("qs_sample_prepare", C.c_void_p(vec.data_ptr()), n, dt, N.QS_SRC_SV, C.c_void_p(ws.data_ptr()), wsb, None)
-    N.call("qs_sample", C.c_void_p(vec.data_ptr()), n, dt, N.QS_SRC_SV, C.c_void_p(ws.data_ptr()), wsb,
+    N.call("qs_sample_prepare", C.c_void_p(vec.data_ptr()), n, dt, src, C.c_void_p(ws.data_ptr()), wsb, None)
+    N.call("qs_sample", C.c_void_p(vec.data_ptr()), n, dt, src, C.c_void_p(ws.data_ptr()), wsb,
            C.c_void_p(u.data_ptr()), shots, mode, C.c_void_p(out.data_ptr()), None)
     return out
 
 
-def _no_alloc(N, vec, n, dt, u, shots, mode):
+def _no_alloc(N, vec, n, dt, u, shots, mode, src=None):
     import torch
+    src = N.QS_SRC_SV if src is None else src
     out = torch.empty(shots, dtype=torch.int64, device="cuda")
-    N.call("qs_sample_noalloc", C.c_void_p(vec.data_ptr()), n, dt, N.QS_SRC_SV, C.c_void_p(u.data_ptr()), shots,
+    N.call("qs_sample_noalloc", C.c_void_p(vec.data_ptr()), n, dt, src, C.c_void_p(u.data_ptr()), shots,
            mode, C.c_void_p(out.data_ptr()), None)
     return out
 
@@ -56,6 +68,29 @@ def test_noalloc_sampling_matches_workspace_entry_point_twice(cuda_ok):
         u = torch.from_numpy(np.random.default_rng(seed + 10).random(shots * per)).cuda()
         want = _with_workspace(lib, N, vec, n, dt, u, shots, mode)
         got = _no_alloc(N, vec, n, dt, u, shots, mode)
+        torch.cuda.synchronize()
+        assert torch.equal(got, want)
+
+
+def test_noalloc_at_its_largest_size_and_on_a_density_matrix(cuda_ok):
+    """n = 26 fills the static tree exactly (2 * 2^16 doubles); a density
+    matrix source reads the diagonal of a 2^n x 2^n array."""
+    import torch
+    from quict_b200 import _native as N
+    lib = N.load()
+    n = N.QS_NOALLOC_SAMPLE_MAX_QUBITS
+    vec = _state(n, 3, np.complex64)
+    u = torch.from_numpy(np.random.default_rng(13).random(8192)).cuda()
+    want = _with_workspace(lib, N, vec, n, N.QS_C64, u, 8192, N.QS_SAMPLE_CDF)
+    got = _no_alloc(N, vec, n, N.QS_C64, u, 8192, N.QS_SAMPLE_CDF)
+    torch.cuda.synchronize()
+    assert torch.equal(got, want)
+    del vec
+    for mode, per in ((N.QS_SAMPLE_CDF, 1), (N.QS_SAMPLE_SEQ, 8)):
+        rho = _density(8, 4, np.complex128)
+        u = torch.from_numpy(np.random.default_rng(14).random(2048 * per)).cuda()
+        want = _with_workspace(lib, N, rho, 8, N.QS_C128, u, 2048, mode, N.QS_SRC_DM)
+        got = _no_alloc(N, rho, 8, N.QS_C128, u, 2048, mode, N.QS_SRC_DM)
         torch.cuda.synchronize()
         assert torch.equal(got, want)
 
