@@ -312,6 +312,8 @@ def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
 
     for _ in range(warmup):
         step()
+    N.jit_wait(600)  # compiled passes ready (no-op with the JIT off)
+    step()
     barrier(ws)
     ms = max_over_ranks(_events_ms(step, steps), ws)
     passes = sum(1 for s in plan_ if isinstance(s, Pass) and s.ops)
@@ -419,13 +421,24 @@ SECTOR = 32  # bytes: the L2 / DRAM sector, the smallest unit a skipped run can 
 
 def op_flops(op):
     """Algorithmic FP64 flops per amplitude of a fused op: a dense m-qubit
-    matrix is 2^m complex multiply-adds per output (8 * 2^m - 2 flops), a
-    diagonal one complex multiply (6) on the entries that are not 1, plain
-    exchanges (X, CX, Swap) none; each control halves the amplitudes touched."""
+    matrix costs, per output, one complex multiply-add (8 flops; the first
+    one a multiply, 6) for each entry of its row that is neither 0 nor +-1,
+    and one complex add (2; none for the first) for each +-1 entry, averaged
+    over the rows; a diagonal one complex multiply (6) on the entries that
+    are not 1; plain exchanges (X, CX, Swap) none; each control halves the
+    amplitudes touched."""
     import numpy as np
     frac = 0.5 ** len(op.cbits)
     if op.kind == "mat":
-        return (8 * (1 << op.m) - 2) * frac
+        m = np.asarray(op.mat)
+        tot = 0.0
+        for row in m:
+            gen = int(np.sum((row != 0) & (row != 1) & (row != -1)))
+            one = int(np.sum((row == 1) | (row == -1)))
+            f = 8 * gen + 2 * one
+            f -= 2 if gen else (2 if one else 0)  # the first term is a product or a copy
+            tot += max(f, 0)
+        return tot / m.shape[0] * frac
     if op.kind == "diag":
         d = np.asarray(op.mat).ravel()
         return 6 * float(np.mean(np.abs(d - 1) > 1e-15)) * frac
@@ -577,10 +590,19 @@ def run_ours(args, ws, rank, local):
                 eng.apply_single(vec, n, st.op)
         eng.run_passes(vec, n, batch)
 
-    for _ in range(args.warmup):
+    # warm-up; passes run as run-time compiled kernels once their compilation
+    # (on host threads, started by the first step) has finished
+    jit0 = N.jit_stats()
+    t_jit = time.perf_counter()
+    device_step()
+    if args.jit:
+        N.jit_wait(600)
+    jit_wall_s = time.perf_counter() - t_jit
+    for _ in range(max(0, args.warmup - 1)):
         device_step()
     torch.cuda.synchronize(dev)
     barrier(ws)
+    jit1 = N.jit_stats()
     launches0 = eng.launches
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
@@ -593,6 +615,14 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     ms = e0.elapsed_time(e1) / args.steps
     launches = (eng.launches - launches0) // args.steps + 1  # + qs_init_zero
+    jit2 = N.jit_stats()
+    jit_info = {"mode": "async" if args.jit else "off",
+                "kernels_compiled": jit1["compiled"] - jit0["compiled"],
+                "compile_ms_host_threads": jit1["compile_ms"] - jit0["compile_ms"],
+                "first_step_wall_s_incl_compile": jit_wall_s,
+                "compiled_launches_per_step": (jit2["compiled_launches"] - jit1["compiled_launches"]) / args.steps,
+                "generic_launches_per_step": (jit2["generic_launches_while_pending"]
+                                              - jit1["generic_launches_while_pending"]) / args.steps}
     ms = max_over_ranks(ms, ws)
     value = ws * len(ops) / (ms / 1e3)
 
@@ -653,6 +683,7 @@ def run_ours(args, ws, rank, local):
                 "d2h_bytes_per_step": 8},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
+        "jit": jit_info,
     }
     if not args.no_extra:
         line["single_gate_sweep"] = gate_sweep(eng, vec, n, ws)
@@ -700,12 +731,16 @@ def main():
     ap.add_argument("--qaoa-instances", type=int, default=512)
     ap.add_argument("--max-pass-cost", type=float, default=None,
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units (default: the tuning cache)")
+    ap.add_argument("--jit", type=int, default=1,
+                    help="1: fused passes run as run-time compiled kernels (compiled during warm-up); 0: generic kernels")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), rank)
         return
     ws, rank, local = dist_init(args)
+    from quict_b200 import _native as N
+    N.jit_set_mode(N.QS_JIT_ASYNC if args.jit else N.QS_JIT_OFF)
     try:
         run_ours(args, ws, rank, local)
     finally:

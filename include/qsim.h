@@ -166,6 +166,48 @@ int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes, int npass
                    const qs_op* ops, int64_t nops_total, const void* mats_dev,
                    int64_t mats_count, void* stream);
 
+/* qs_apply_fused with the matrix table also given in HOST memory (the same
+ * values as mats_dev, in the state's precision).  A register pass then runs
+ * as a kernel generated for that pass alone and compiled at run time
+ * (NVRTC, sm_100a) when the library's JIT mode allows it: its ops, slot
+ * masks and relayout addresses are constants of the code, plain exchanges
+ * are register renamings, and its matrices travel in the launch's parameter
+ * block (read as constant-bank operands).  Compiled kernels are cached by
+ * their source, which depends on the pass's structure and on which matrix
+ * entries are exactly 0, 1 or -1, not on the other values.  Until a pass's
+ * kernel is compiled (mode QS_JIT_ASYNC) the generic kernel runs it, with
+ * the same results.  mats_host may be NULL (the generic kernels only).
+ * No counterpart in the reference, which launches one kernel per gate. */
+int qs_apply_fused_ex(void* vec, int n, int dtype, const qs_pass* passes, int npasses,
+                      const qs_op* ops, int64_t nops_total, const void* mats_dev,
+                      const void* mats_host, int64_t mats_count, void* stream);
+
+/* ---- run-time compiled passes ------------------------------------------------ */
+#define QS_JIT_OFF   0    /* generic fused kernels only                             */
+#define QS_JIT_ASYNC 1    /* compile on host threads; generic kernels meanwhile (default;
+                             the QS_JIT environment variable sets the initial mode) */
+#define QS_JIT_SYNC  2    /* compile before the first launch of a new pass shape    */
+/* Set the mode; returns the previous one (or a negative error). */
+int qs_jit_set_mode(int mode);
+/* Wait until no compilation is queued or running (timeout_s < 0: no limit);
+ * QS_ETIMEOUT when the limit passes first. */
+int qs_jit_wait(double timeout_s);
+/* out[0..n-1] <- kernels compiled, compilations failed, compilations pending,
+ * launches of compiled kernels, launches that ran the generic kernel while a
+ * compilation was pending, total compile milliseconds, cache hits. */
+int qs_jit_stats(int64_t* out, int n);
+/* Log of the last failed compilation or load ("" if none). */
+const char* qs_jit_last_log(void);
+/* Compile `src` with NVRTC only (no device needed); *cubin_bytes <- size. */
+int qs_jit_compile_check(const char* src, int64_t* cubin_bytes);
+/* The generated source of launch `launch_index` of one register pass (as
+ * qs_apply_fused_ex would plan it), without a device: *src_len <- its
+ * length; up to out_size - 1 bytes are copied to `out` (may be NULL).
+ * QS_ENOTSUP for passes that do not run as generated kernels. */
+int qs_jit_pass_source(int n, int dtype, const qs_pass* pass, const qs_op* ops, int64_t nops_total,
+                       const void* mats_host, int64_t mats_count, int launch_index, char* out,
+                       size_t out_size, int64_t* src_len);
+
 /* ---- differentiation / observables ---------------------------------------- */
 /* Backward-sweep pass of the adjoint method: every QS_OP_MAT / DIAG / ANTI /
  * SWAP op is applied to BOTH psi and lam (the caller passes the inverse

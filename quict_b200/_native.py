@@ -28,6 +28,9 @@ QS_SAMPLE_CDF, QS_SAMPLE_SEQ = 0, 1
 QS_MAX_TILE_BITS = 14
 QS_MAX_PASS_OPS = 160
 QS_NOALLOC_SAMPLE_MAX_QUBITS = 26
+QS_JIT_OFF, QS_JIT_ASYNC, QS_JIT_SYNC = 0, 1, 2
+JIT_STAT_KEYS = ("compiled", "failed", "pending", "compiled_launches", "generic_launches_while_pending",
+                 "compile_ms", "cache_hits")
 
 
 class NativeLibraryError(RuntimeError):
@@ -104,6 +107,14 @@ SIGNATURES = {
     "qs_sample": (_i, [_vp, _i, _i, _i, _vp, _sz, _vp, _i64, _i, _vp, _vp]),
     "qs_histogram": (_i, [_vp, _i64, _vp, _i64, _vp]),
     "qs_sample_noalloc": (_i, [_vp, _i, _i, _i, _vp, _i64, _i, _vp, _vp]),
+    "qs_apply_fused_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp]),
+    "qs_jit_set_mode": (_i, [_i]),
+    "qs_jit_wait": (_i, [_d]),
+    "qs_jit_stats": (_i, [C.POINTER(C.c_int64), _i]),
+    "qs_jit_last_log": (C.c_char_p, []),
+    "qs_jit_compile_check": (_i, [C.c_char_p, C.POINTER(C.c_int64)]),
+    "qs_jit_pass_source": (_i, [_i, _i, C.POINTER(qs_pass), C.POINTER(qs_op), _i64, _vp, _i64, _i, C.c_char_p, _sz,
+                                C.POINTER(C.c_int64)]),
 }
 
 _lib = None
@@ -151,3 +162,20 @@ def stream_ptr(stream) -> int | None:
     if stream is None:
         return None
     return int(stream.cuda_stream) or None
+
+
+def jit_set_mode(mode: int) -> int:
+    """Set libqsim's run-time compilation mode (QS_JIT_OFF / ASYNC / SYNC);
+    returns the previous mode."""
+    return call("qs_jit_set_mode", int(mode))
+
+
+def jit_wait(timeout_s: float = -1.0) -> None:
+    """Block until every queued pass compilation has finished."""
+    call("qs_jit_wait", float(timeout_s))
+
+
+def jit_stats() -> dict:
+    out = (C.c_int64 * len(JIT_STAT_KEYS))()
+    call("qs_jit_stats", out, len(JIT_STAT_KEYS))
+    return dict(zip(JIT_STAT_KEYS, (int(v) for v in out)))

@@ -24,11 +24,15 @@
 // (statevector_simulator.py:155-164, gate_function.py:31-1031).
 #include <algorithm>
 #include <array>
+#include <cstdarg>
+#include <cstring>
+#include <string>
 #include <type_traits>
 #include <utility>
 #include <vector>
 
 #include "common.cuh"
+#include "jit.h"
 
 namespace qs {
 namespace {
@@ -1370,8 +1374,350 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
     return ndone;
 }
 
+// ------------------------------------------------------- run-time compiled passes
+// A register pass planned by build_reg can also run as a kernel generated for
+// it alone: every op, slot mask, control and relayout address is a constant
+// of the generated code, so there is no per-op dispatch, plain exchanges
+// (X, CX, SWAP without outside controls) become register renamings, zero and
+// unit matrix entries drop out of the arithmetic, and the matrices are read
+// as constant-bank operands from the launch's parameter block.  The source
+// depends on the pass's structure and on which matrix entries are exactly
+// 0, 1 or -1, not on the other matrix values, so passes of the same shape
+// share one compiled kernel (jit.cu caches by source text).
+struct JitPass {
+    std::string src;
+    std::vector<uint64_t> params;  // the kernel's parameter block (16-byte multiple)
+    int threads = 0;
+    size_t smem = 0;
+};
+
+constexpr size_t kJitMaxParamBytes = 32000;  // below the 32764-byte kernel parameter limit
+
+struct SrcBuf {
+    std::string s;
+    void add(const char* fmt, ...) __attribute__((format(printf, 2, 3))) {
+        char tmp[1024];
+        va_list ap;
+        va_start(ap, fmt);
+        int k = vsnprintf(tmp, sizeof(tmp), fmt, ap);
+        va_end(ap);
+        if (k >= int(sizeof(tmp))) k = int(sizeof(tmp)) - 1;
+        s.append(tmp, size_t(k));
+    }
+};
+
+// XOR of per-thread-bit images over the set bits of threadIdx.x, as an expression
+std::string thread_xor_expr(const uint32_t* img, int nT) {
+    std::string e;
+    for (int i = 0; i < nT; ++i) {
+        if (!img[i]) continue;
+        char t[64];
+        snprintf(t, sizeof(t), "%s(((tid >> %d) & 1u) * %uu)", e.empty() ? "" : " ^ ", i, img[i]);
+        e += t;
+    }
+    return e.empty() ? std::string("0u") : e;
+}
+
+template <typename V>
+bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
+    constexpr bool C128 = sizeof(V) == 16;
+    const int E = 1 << R, nT = a.nT, K = a.K, L = a.L, H = a.H;
+    const int threads = 1 << nT;
+    const int NM = a.nmats > 0 ? a.nmats : 1;
+    const int NOPS = a.nops > 0 ? a.nops : 1;
+    // ---- parameter block: V m[NM]; u64 ntiles, gthr[8], gslot[E], hibit[16], gctrl[NOPS], hsh[4 NOPS]
+    const size_t off_u64 = sizeof(V) * size_t(NM);
+    const size_t o_ntiles = off_u64, o_gthr = o_ntiles + 8, o_gslot = o_gthr + 64, o_hibit = o_gslot + 8 * E,
+                 o_gctrl = o_hibit + 128, o_hsh = o_gctrl + 8 * size_t(NOPS);
+    size_t bytes = o_hsh + 32 * size_t(NOPS);
+    bytes = (bytes + 15) & ~size_t(15);
+    if (bytes > kJitMaxParamBytes) return false;
+    out.params.assign(bytes / 8, 0);
+    unsigned char* pb = reinterpret_cast<unsigned char*>(out.params.data());
+    auto put64 = [&](size_t off, uint64_t v) { memcpy(pb + off, &v, 8); };
+    // matrices in slot order, exactly as the generic kernel stages them
+    V* pm = reinterpret_cast<V*>(pb);
+    for (int o = 0; o < a.nops; ++o) {
+        const KCopy& c = a.cp[o];
+        const int D = 1 << c.m;
+        const int cnt = c.diag ? D : D * D;
+        for (int e = 0; e < cnt; ++e) {
+            const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
+            int sr = 0, sc = 0;
+            for (int i = 0; i < c.m; ++i) {
+                sr |= ((kr >> i) & 1) << c.perm[i];
+                sc |= ((kc >> i) & 1) << c.perm[i];
+            }
+            pm[c.soff + e] = hm[c.goff + (c.diag ? sr : sr * D + sc)];
+        }
+    }
+    auto gbit = [&](int b) -> uint64_t { return uint64_t(1) << (b < L ? b : a.hi[b - L]); };
+    const KStage& SL = a.st[a.nstages - 1];
+    put64(o_ntiles, uint64_t(1) << (a.n - K));
+    for (int i = 0; i < nT; ++i) put64(o_gthr + 8 * i, gbit(SL.T[i]));
+    for (int s = 0; s < E; ++s) {
+        uint64_t v = 0;
+        for (int j = 0; j < R; ++j)
+            if ((s >> j) & 1) v |= gbit(SL.R[j]);
+        put64(o_gslot + 8 * s, v);
+    }
+    for (int t = 0; t < H; ++t) put64(o_hibit + 8 * t, uint64_t(1) << a.hi[t]);
+    for (int o = 0; o < a.nops; ++o) {
+        put64(o_gctrl + 8 * o, a.ops[o].gctrl);
+        for (int q = 0; q < a.ops[o].nh; ++q)
+            put64(o_hsh + 32 * o + 8 * q, a.ops[o].hsrc[q] >= 64 ? uint64_t(a.ops[o].hsrc[q] - 64) : 0);
+    }
+    // value class of a parameter-block entry: 0, 1, -1 or general
+    auto vclass = [&](int idx) -> int {
+        const V v = pm[idx];
+        if (v.y != 0) return 3;
+        if (v.x == 0) return 0;
+        if (v.x == 1) return 1;
+        if (v.x == -1) return 2;
+        return 3;
+    };
+    const char* VT = C128 ? "double2" : "float2";
+    const char* MK = C128 ? "make_double2" : "make_float2";
+    const char* FMA = C128 ? "__fma_rn" : "__fmaf_rn";
+    const int target = C128 ? 384 : 512;
+    const int minb = threads >= target ? 1 : target / threads;
+    SrcBuf g;
+    g.add("// generated fused pass: n=%d K=%d L=%d R=%d stages=%d ops=%d\n", a.n, K, L, R, a.nstages, a.nops);
+    g.add("typedef unsigned long long u64;\ntypedef unsigned int u32;\ntypedef %s V;\n", VT);
+    g.add("static __device__ __forceinline__ V cmul(V a, V b) { V r; r.x = a.x * b.x - a.y * b.y; "
+          "r.y = a.x * b.y + a.y * b.x; return r; }\n");
+    g.add("static __device__ __forceinline__ V cfma(V a, V b, V c) { V r; r.x = %s(a.x, b.x, %s(-a.y, b.y, c.x)); "
+          "r.y = %s(a.x, b.y, %s(a.y, b.x, c.y)); return r; }\n", FMA, FMA, FMA, FMA);
+    g.add("static __device__ __forceinline__ V cadd(V a, V b) { V r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }\n");
+    g.add("static __device__ __forceinline__ V cneg(V a) { V r; r.x = -a.x; r.y = -a.y; return r; }\n");
+    g.add("static __device__ __forceinline__ V csel(bool c, V a, V b) { V r; r.x = c ? a.x : b.x; "
+          "r.y = c ? a.y : b.y; return r; }\n");
+    g.add("struct __align__(16) P { V m[%d]; u64 ntiles; u64 gthr[8]; u64 gslot[%d]; u64 hibit[16]; u64 gctrl[%d]; "
+          "u64 hsh[%d]; };\n", NM, E, NOPS, 4 * NOPS);
+    g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
+          "const __grid_constant__ P p) {\n", threads, minb);
+    g.add("  extern __shared__ __align__(16) unsigned char smem_raw[];\n");
+    g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", 1u << K);
+    g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
+    g.add("  const u32 tid = threadIdx.x;\n");
+    g.add("  for (u32 j = tid; j < %du; j += %du) { u64 o = 0;\n", 1u << H, threads);
+    g.add("#pragma unroll\n    for (int t = 0; t < %d; ++t) if ((j >> t) & 1u) o |= p.hibit[t];\n    hoff[j] = o; }\n", H);
+    g.add("  u64 gthr = 0;\n");
+    for (int i = 0; i < nT; ++i) g.add("  if ((tid >> %d) & 1u) gthr |= p.gthr[%d];\n", i, i);
+    // per-stage thread images
+    for (int si = 0; si < a.nstages; ++si) {
+        const KStage& S = a.st[si];
+        uint32_t rt[8], wt[8], tb[8];
+        for (int i = 0; i < 8; ++i) {
+            rt[i] = S.rthr[i];
+            wt[i] = S.wthr[i];
+            tb[i] = S.tbit[i];
+        }
+        g.add("  const u32 RD%d = %s;\n", si, thread_xor_expr(rt, nT).c_str());
+        if (si > 0) g.add("  const u32 WR%d = %s;\n", si, thread_xor_expr(wt, nT).c_str());
+        g.add("  const u32 TH%d = %s;\n", si, thread_xor_expr(tb, nT).c_str());
+    }
+    g.add("  __syncthreads();\n");
+    g.add("  const u64 ntiles = p.ntiles;\n  const u64 tstep = gridDim.x;\n  u64 tile = blockIdx.x;\n");
+    g.add("  auto tile_base = [&](u64 t) -> u64 { u64 b = t << %d;\n", L);
+    g.add("#pragma unroll\n    for (int i = 0; i < %d; ++i) { const u64 lo = p.hibit[i] - 1ull; "
+          "b = ((b & ~lo) << 1) | (b & lo); }\n    return b; };\n", H);
+    const int EPC = 16 / int(sizeof(V));
+    g.add("  auto prefetch = [&](V* dst, u64 base) {\n");
+    g.add("    for (u32 c = tid; c < %du; c += %du) { const u32 e = c * %du;\n", (1u << K) / EPC, threads, EPC);
+    g.add("      const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst + e));\n");
+    g.add("      asm volatile(\"cp.async.cg.shared.global [%%0], [%%1], 16;\\n\" :: \"r\"(sa), "
+          "\"l\"(vec + (base | hoff[e >> %d] | (e & %du))) : \"memory\"); }\n", L, (1u << L) - 1u);
+    g.add("    asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\"); };\n");
+    g.add("  if (tile < ntiles) prefetch(b0, tile_base(tile));\n");
+    g.add("  for (u32 it = 0; tile < ntiles; ++it, tile += tstep) {\n");
+    g.add("    V* const cur = (it & 1u) ? b1 : b0;\n    const u64 base = tile_base(tile);\n");
+    g.add("    asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n    __syncthreads();\n");
+    g.add("    if (tile + tstep < ntiles) prefetch((it & 1u) ? b0 : b1, tile_base(tile + tstep));\n");
+    // ---- body
+    int fresh = 0;
+    std::vector<int> var(E);  // slot -> SSA value id
+    auto slot_addr = [&](const uint16_t* img, int s) {
+        uint32_t c = 0;
+        for (int j = 0; j < R; ++j)
+            if ((s >> j) & 1) c ^= img[j];
+        return c;
+    };
+    for (int s = 0; s < E; ++s) {
+        var[s] = fresh++;
+        g.add("    const V v%d = cur[RD0 ^ %uu];\n", var[s], slot_addr(a.st[0].rslot, s));
+    }
+    for (int si = 0; si < a.nstages; ++si) {
+        const KStage& S = a.st[si];
+        if (si > 0) {
+            g.add("    __syncthreads();\n");
+            for (int s = 0; s < E; ++s) g.add("    cur[WR%d ^ %uu] = v%d;\n", si, slot_addr(S.wslot, s), var[s]);
+            g.add("    __syncthreads();\n");
+            for (int s = 0; s < E; ++s) {
+                var[s] = fresh++;
+                g.add("    const V v%d = cur[RD%d ^ %uu];\n", var[s], si, slot_addr(S.rslot, s));
+            }
+        }
+        for (int o = S.op_begin; o < S.op_begin + S.op_count; ++o) {
+            const KOp& op = a.ops[o];
+            std::string cond;
+            if (op.gctrl) {
+                char t[96];
+                snprintf(t, sizeof(t), "((base & p.gctrl[%d]) == p.gctrl[%d])", o, o);
+                cond = t;
+            }
+            if (op.tctrl) {
+                char t[96];
+                snprintf(t, sizeof(t), "%s((TH%d & %uu) == %uu)", cond.empty() ? "" : " && ", si, unsigned(op.tctrl),
+                         unsigned(op.tctrl));
+                cond += t;
+            }
+            const int scm = op.scm;
+            auto ctrl_ok = [&](int s) { return (s & scm) == scm; };
+            if (op.code == QS_OP_MAT) {
+                const int mask = op.mask, M = popc_c(mask), D = 1 << M;
+                std::vector<std::pair<int, int>> groups;  // (s, first new id)
+                g.add("    // op %d: dense on slot mask %d%s\n", o, mask, cond.empty() ? "" : " (controlled)");
+                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
+                for (int s = 0; s < E; ++s) {
+                    if ((s & mask) || !ctrl_ok(s)) continue;
+                    int in[16];
+                    for (int c = 0; c < D; ++c) in[c] = var[s | pdep_c(c, mask)];
+                    int outid[16];
+                    for (int r = 0; r < D; ++r) {
+                        std::string e;
+                        for (int c = 0; c < D; ++c) {
+                            const int idx = op.moff + r * D + c;
+                            const int cl = vclass(idx);
+                            if (cl == 0) continue;
+                            char t[160];
+                            if (e.empty()) {
+                                if (cl == 1) snprintf(t, sizeof(t), "v%d", in[c]);
+                                else if (cl == 2) snprintf(t, sizeof(t), "cneg(v%d)", in[c]);
+                                else snprintf(t, sizeof(t), "cmul(p.m[%d], v%d)", idx, in[c]);
+                                e = t;
+                            } else {
+                                if (cl == 1) snprintf(t, sizeof(t), "cadd(%s, v%d)", e.c_str(), in[c]);
+                                else if (cl == 2) snprintf(t, sizeof(t), "cadd(%s, cneg(v%d))", e.c_str(), in[c]);
+                                else snprintf(t, sizeof(t), "cfma(p.m[%d], v%d, %s)", idx, in[c], e.c_str());
+                                e = t;
+                            }
+                        }
+                        if (e.empty()) {
+                            char t[64];
+                            snprintf(t, sizeof(t), "%s(0, 0)", MK);
+                            e = t;
+                        }
+                        outid[r] = fresh++;
+                        if (cond.empty()) g.add("    const V v%d = %s;\n", outid[r], e.c_str());
+                        else g.add("    const V v%d = c%d ? %s : v%d;\n", outid[r], o, e.c_str(), in[r]);
+                    }
+                    for (int r = 0; r < D; ++r) var[s | pdep_c(r, mask)] = outid[r];
+                }
+            } else if (op.code == QS_OP_ANTI || op.code == QS_OP_SWAP) {  // plain exchanges
+                int b0, b1;
+                if (op.code == QS_OP_ANTI) {
+                    b0 = 0;
+                    b1 = op.mask;
+                } else {
+                    b0 = 1 << nth_bit(op.mask, 0);
+                    b1 = 1 << nth_bit(op.mask, 1);
+                }
+                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
+                for (int s = 0; s < E; ++s) {
+                    if ((s & op.mask) || !ctrl_ok(s)) continue;
+                    const int x0 = var[s | b0], x1 = var[s | b1];
+                    if (cond.empty()) {
+                        var[s | b0] = x1;
+                        var[s | b1] = x0;
+                    } else {
+                        const int n0 = fresh++, n1 = fresh++;
+                        g.add("    const V v%d = csel(c%d, v%d, v%d);\n", n0, o, x1, x0);
+                        g.add("    const V v%d = csel(c%d, v%d, v%d);\n", n1, o, x0, x1);
+                        var[s | b0] = n0;
+                        var[s | b1] = n1;
+                    }
+                }
+            } else if (op.code == QS_OP_DIAG) {
+                g.add("    // op %d: diagonal, %d register bits, %d other bits\n", o, op.ns, op.nh);
+                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
+                if (op.nh > 0) {
+                    std::string h;
+                    for (int q = 0; q < op.nh; ++q) {
+                        char t[128];
+                        const int src = op.hsrc[q];
+                        if (src < 64) snprintf(t, sizeof(t), "((TH%d >> %d) & 1u)", si, src);
+                        else snprintf(t, sizeof(t), "u32((base >> p.hsh[%d]) & 1ull)", 4 * o + q);
+                        h = h.empty() ? std::string(t) : "((" + h + ") << 1) | " + t;
+                    }
+                    g.add("    const u32 h%d = %s;\n", o, h.c_str());
+                }
+                for (int s = 0; s < E; ++s) {
+                    if (!ctrl_ok(s)) continue;
+                    const int k = op.kidx[s];
+                    std::string e;
+                    char t[160];
+                    if (op.nh == 0) {
+                        const int idx = op.moff + k;
+                        const int cl = vclass(idx);
+                        if (cl == 1) continue;
+                        if (cl == 2) snprintf(t, sizeof(t), "cneg(v%d)", var[s]);
+                        else if (cl == 0) snprintf(t, sizeof(t), "%s(0, 0)", MK);
+                        else snprintf(t, sizeof(t), "cmul(v%d, p.m[%d])", var[s], idx);
+                    } else {
+                        snprintf(t, sizeof(t), "cmul(v%d, p.m[%d + ((h%d << %d) | %du)])", var[s], int(op.moff), o,
+                                 int(op.ns), k);
+                    }
+                    e = t;
+                    const int nid = fresh++;
+                    if (cond.empty()) g.add("    const V v%d = %s;\n", nid, e.c_str());
+                    else g.add("    const V v%d = c%d ? %s : v%d;\n", nid, o, e.c_str(), var[s]);
+                    var[s] = nid;
+                }
+            } else {
+                return false;  // EXPECT ops are not generated
+            }
+        }
+    }
+    for (int s = 0; s < E; ++s) g.add("    vec[base | gthr | p.gslot[%d]] = v%d;\n", s, var[s]);
+    g.add("  }\n}\n");
+    out.src.swap(g.s);
+    out.threads = threads;
+    out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * (size_t(1) << H);
+    return true;
+}
+
+// Launch the run-time compiled kernel of a planned register pass, if the
+// compiler has it ready (mode SYNC: after compiling it); returns 1 when it
+// was launched, 0 when the generic kernel has to run, < 0 on error.
+template <typename V>
+int launch_jit(V* vec, const RegArgs& args, int R, const V* hm, cudaStream_t st) {
+    const int jm = jit::mode();
+    if (jm == QS_JIT_OFF || hm == nullptr || args.batched || args.nexp > 0) return 0;
+    static thread_local JitPass jp;
+    if (!gen_reg_pass<V>(args, R, hm, jp)) return 0;
+    void* fn = jit::lookup(jp.src, "qs_pass", jm == QS_JIT_SYNC);
+    if (fn == nullptr) {
+        jit::count_launch(false);
+        return 0;
+    }
+    int occ = 0;
+    int rc = jit::occupancy(fn, jp.threads, jp.smem, &occ);
+    if (rc) return rc;
+    if (occ < 1) occ = 1;
+    const uint64_t ntiles = uint64_t(1) << (args.n - args.K);
+    const uint64_t cap = uint64_t(sm_count()) * uint64_t(occ);
+    void* vp = vec;
+    void* params[] = {&vp, jp.params.data()};
+    rc = jit::launch(fn, unsigned(ntiles < cap ? ntiles : cap), unsigned(jp.threads), jp.smem, st, params);
+    if (rc) return rc;
+    jit::count_launch(true);
+    return 1;
+}
+
 template <typename V, int R, bool EXP, bool BIG>
-int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
+int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st,
+                 const V* hm = nullptr) {
     static thread_local RegArgs args;
     config_smem((const void*)k_fused_reg<V, R, EXP, BIG>);
     std::vector<int> rem(ps.op_count);
@@ -1383,6 +1729,11 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
         if (used <= 0) {
             set_error("qs_apply_fused: op %d does not fit a register tile", next);
             return QS_EINVAL;
+        }
+        if (!EXP) {
+            int jr = launch_jit<V>(vec, args, R, hm, st);
+            if (jr < 0) return jr;
+            if (jr == 1) continue;
         }
         const int threads = 1 << (ps.k - R);
         size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + args.nmats) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
@@ -1409,7 +1760,8 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
 // variant (adjoint pair passes take dense ops on at most 2 bits; their BIG
 // variant only adds the controlled paths).
 template <typename V, int R, bool EXP>
-int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st) {
+int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st,
+               const V* hm = nullptr) {
     bool big = false;
     for (int i = 0; i < ps.op_count; ++i) {
         const qs_op& op = ops[ps.op_begin + i];
@@ -1433,8 +1785,8 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
         return big ? launch_reg_k<V, R, true, true>(vec, n, ps, ops, mats, partials, st)
                    : launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st);
     } else {
-        return big ? launch_reg_k<V, R, false, true>(vec, n, ps, ops, mats, partials, st)
-                   : launch_reg_k<V, R, false, false>(vec, n, ps, ops, mats, partials, st);
+        return big ? launch_reg_k<V, R, false, true>(vec, n, ps, ops, mats, partials, st, hm)
+                   : launch_reg_k<V, R, false, false>(vec, n, ps, ops, mats, partials, st, hm);
     }
 }
 
@@ -1442,13 +1794,14 @@ template <typename V>
 constexpr int reg_bits() { return sizeof(V) == 16 ? 4 : 5; }
 
 template <typename V>
-int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st) {
+int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, cudaStream_t st,
+                const V* hm = nullptr) {
     constexpr int R = reg_bits<V>();
     const int nT = ps.k - R;
     const size_t smem = sizeof(V) * (2 * (size_t(1) << ps.k) + QS_MAX_PASS_MATS) + 8 * ((size_t(1) << (ps.k - ps.nlow)) + (1 << R)) +
                         sizeof(KOp) * QS_MAX_PASS_OPS + 16 + sizeof(KStage) * kMaxStages + QS_MAX_PASS_MATS;
     if (nT >= 5 && nT <= 8 && ps.nlow >= 5 && smem <= size_t(smem_optin()))
-        return launch_reg<V, R, false>(vec, n, ps, ops, mats, nullptr, st);
+        return launch_reg<V, R, false>(vec, n, ps, ops, mats, nullptr, st, hm);
     return launch_smem<V, false>(vec, nullptr, n, ps, ops, mats, nullptr, st);
 }
 
@@ -1459,6 +1812,12 @@ using namespace qs;
 
 extern "C" int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes, int npasses, const qs_op* ops,
                               int64_t nops_total, const void* mats_dev, int64_t mats_count, void* stream) {
+    return qs_apply_fused_ex(vec, n, dtype, passes, npasses, ops, nops_total, mats_dev, nullptr, mats_count, stream);
+}
+
+extern "C" int qs_apply_fused_ex(void* vec, int n, int dtype, const qs_pass* passes, int npasses, const qs_op* ops,
+                                 int64_t nops_total, const void* mats_dev, const void* mats_host, int64_t mats_count,
+                                 void* stream) {
     QS_REQUIRE(vec != nullptr, "null state vector");
     QS_REQUIRE(n >= 1 && n <= 40, "qubit count %d outside [1, 40]", n);
     QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
@@ -1475,8 +1834,10 @@ extern "C" int qs_apply_fused(void* vec, int n, int dtype, const qs_pass* passes
     for (int i = 0; i < npasses; ++i) {
         if (passes[i].op_count == 0) continue;
         int rc = dtype == QS_C128
-                     ? launch_pass<double2>((double2*)vec, n, passes[i], ops, (const double2*)mats_dev, as_stream(stream))
-                     : launch_pass<float2>((float2*)vec, n, passes[i], ops, (const float2*)mats_dev, as_stream(stream));
+                     ? launch_pass<double2>((double2*)vec, n, passes[i], ops, (const double2*)mats_dev,
+                                            as_stream(stream), (const double2*)mats_host)
+                     : launch_pass<float2>((float2*)vec, n, passes[i], ops, (const float2*)mats_dev,
+                                           as_stream(stream), (const float2*)mats_host);
         if (rc) return rc;
     }
     return QS_OK;
@@ -1541,6 +1902,52 @@ extern "C" int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* pa
                                                                     (const float2*)mats_dev, partials_dev,
                                                                     as_stream(stream));
         if (rc) return rc;
+    }
+    return QS_OK;
+}
+
+extern "C" int qs_jit_pass_source(int n, int dtype, const qs_pass* pass, const qs_op* ops, int64_t nops_total,
+                                  const void* mats_host, int64_t mats_count, int launch_index, char* out,
+                                  size_t out_size, int64_t* src_len) {
+    QS_REQUIRE(n >= 1 && n <= 40, "qubit count %d outside [1, 40]", n);
+    QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
+    QS_REQUIRE(pass != nullptr && mats_host != nullptr && src_len != nullptr, "null argument");
+    QS_REQUIRE(launch_index >= 0, "negative launch index");
+    int rc = validate_pass(*pass, n, ops, nops_total, mats_count);
+    if (rc) return rc;
+    const int R = dtype == QS_C128 ? reg_bits<double2>() : reg_bits<float2>();
+    const int nT = pass->k - R;
+    if (!(nT >= 5 && nT <= 8 && pass->nlow >= 5)) {
+        set_error("qs_jit_pass_source: tile 2^%d / nlow %d is not a register tile", pass->k, pass->nlow);
+        return QS_ENOTSUP;
+    }
+    static thread_local RegArgs args;
+    std::vector<int> rem(pass->op_count);
+    for (int i = 0; i < pass->op_count; ++i) rem[i] = i;
+    JitPass jp;
+    bool ok = false;
+    for (int li = 0; li <= launch_index; ++li) {
+        if (rem.empty()) {
+            set_error("qs_jit_pass_source: the pass has %d launches", li);
+            return QS_EINVAL;
+        }
+        if (build_reg(*pass, ops, rem, n, R, dtype == QS_C128 ? 3 : 4, args) <= 0) {
+            set_error("qs_jit_pass_source: an op does not fit a register tile");
+            return QS_EINVAL;
+        }
+        if (li == launch_index)
+            ok = dtype == QS_C128 ? gen_reg_pass<double2>(args, R, (const double2*)mats_host, jp)
+                                  : gen_reg_pass<float2>(args, R, (const float2*)mats_host, jp);
+    }
+    if (!ok) {
+        set_error("qs_jit_pass_source: this launch is not generated (batched, EXPECT ops or parameters too large)");
+        return QS_ENOTSUP;
+    }
+    *src_len = int64_t(jp.src.size());
+    if (out != nullptr && out_size > 0) {
+        const size_t k = jp.src.size() < out_size - 1 ? jp.src.size() : out_size - 1;
+        memcpy(out, jp.src.data(), k);
+        out[k] = 0;
     }
     return QS_OK;
 }

@@ -1,0 +1,48 @@
+// Run-time compiled kernels: CUDA source generated for one fused pass is
+// compiled by NVRTC for sm_100a and loaded with the driver API, per device.
+// NVRTC and the driver library are opened with dlopen on first use, so
+// libqsim.so itself links against neither (it loads on hosts without a GPU).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace qs {
+namespace jit {
+
+// QS_JIT_OFF / QS_JIT_ASYNC / QS_JIT_SYNC (include/qsim.h)
+int mode();
+void set_mode(int m);
+
+// Kernel `name` of `src`, loaded on the current device: non-null when ready.
+// A source seen for the first time is queued for compilation on the pool
+// (mode ASYNC: the call returns null until it is done) or compiled before
+// returning (mode SYNC, or `block`).  Null when compilation failed; the
+// first failure's log is kept for qs_jit_last_log.
+void* lookup(const std::string& src, const char* name, bool block);
+
+// cuLaunchKernel of a looked-up function; `params` points to the kernel's
+// parameter values (one pointer per kernel argument).
+int launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st, void** params);
+
+// Resident blocks per SM for `fn` at `block` threads and `smem` dynamic
+// shared memory (after opting it into that much shared memory).
+int occupancy(void* fn, int block, size_t smem, int* out);
+
+// Wait for every queued compilation (seconds; < 0: no limit).  QS_ETIMEOUT
+// when the limit passed first.
+int wait_all(double timeout_s);
+
+// Counters: [0] kernels compiled, [1] compilations failed, [2] queued or
+// running, [3] launches of compiled kernels, [4] launches that fell back to
+// the generic kernel while a compilation was pending, [5] total compile
+// milliseconds, [6] cache hits on a compiled kernel.
+void stats(int64_t* out, int n);
+void count_launch(bool compiled);
+const char* last_log();
+
+}  // namespace jit
+}  // namespace qs

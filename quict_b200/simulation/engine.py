@@ -152,9 +152,10 @@ class Engine:
         # host behind kernels already in flight
         mats = torch.from_numpy(host).pin_memory().to(self.device, non_blocking=True)
         self.h2d_bytes += mats.numel() * mats.element_size()
+        hp = C.c_void_p(host.ctypes.data)  # the same table on the host: generated passes take it as parameters
         if self.pass_events is None:
-            N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), cps, npass, cops, nops,
-                   C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+            N.call("qs_apply_fused_ex", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), cps, npass, cops, nops,
+                   C.c_void_p(mats.data_ptr()), hp, int(mats.numel()), self.stream)
         else:
             # one call per pass, bracketed by CUDA events on the launching stream
             stream = torch.cuda.current_stream(self.device)
@@ -162,8 +163,8 @@ class Engine:
                 if passes[i].ops:
                     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                     a.record(stream)
-                N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), C.byref(cps[i]), 1,
-                       cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+                N.call("qs_apply_fused_ex", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), C.byref(cps[i]), 1,
+                       cops, nops, C.c_void_p(mats.data_ptr()), hp, int(mats.numel()), self.stream)
                 if passes[i].ops:
                     b.record(stream)
                     self.pass_events.append((a, b, len(passes[i].ops)))

@@ -127,9 +127,11 @@ def test_dm_gpu_matches_reference_fixture(cuda_ok, n, fusion):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [7, 12])
+@pytest.mark.parametrize("n", [7])
 def test_dm_config2_style_vs_oracle(cuda_ok, n):
-    """150-gate config-0 gate set with composed damping+depolarizing per gate."""
+    """150-gate config-0 gate set with composed damping+depolarizing per gate,
+    against the Kraus-sum oracle (the 12-qubit run is checked in full against
+    the superoperator oracle in test_benchmark_sizes.py)."""
     from quict_b200.core import Circuit
     from quict_b200.simulation import DensityMatrixSimulator
     size = 150 if n == 7 else 12
