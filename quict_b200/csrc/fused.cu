@@ -1395,13 +1395,17 @@ constexpr size_t kJitMaxParamBytes = 32000;  // below the 32764-byte kernel para
 
 struct SrcBuf {
     std::string s;
+    bool truncated = false;  // a formatted piece did not fit: the source is not used
     void add(const char* fmt, ...) __attribute__((format(printf, 2, 3))) {
         char tmp[1024];
         va_list ap;
         va_start(ap, fmt);
         int k = vsnprintf(tmp, sizeof(tmp), fmt, ap);
         va_end(ap);
-        if (k >= int(sizeof(tmp))) k = int(sizeof(tmp)) - 1;
+        if (k >= int(sizeof(tmp))) {
+            truncated = true;
+            k = int(sizeof(tmp)) - 1;
+        }
         s.append(tmp, size_t(k));
     }
 };
@@ -1467,19 +1471,29 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
         for (int q = 0; q < a.ops[o].nh; ++q)
             put64(o_hsh + 32 * o + 8 * q, a.ops[o].hsrc[q] >= 64 ? uint64_t(a.ops[o].hsrc[q] - 64) : 0);
     }
-    // value class of a parameter-block entry: 0, 1, -1 or general
+    // value class of a parameter-block entry: 0, 1, -1, general (3), real (4),
+    // imaginary (5); a real or imaginary entry multiplies with two products
+    // instead of four
     auto vclass = [&](int idx) -> int {
         const V v = pm[idx];
-        if (v.y != 0) return 3;
-        if (v.x == 0) return 0;
-        if (v.x == 1) return 1;
-        if (v.x == -1) return 2;
-        return 3;
+        if (v.y == 0) {
+            if (v.x == 0) return 0;
+            if (v.x == 1) return 1;
+            if (v.x == -1) return 2;
+            return 4;
+        }
+        return v.x == 0 ? 5 : 3;
     };
     const char* VT = C128 ? "double2" : "float2";
     const char* MK = C128 ? "make_double2" : "make_float2";
     const char* FMA = C128 ? "__fma_rn" : "__fmaf_rn";
-    const int target = C128 ? 384 : 512;
+    // resident threads per SM the register budget is sized for (launch bounds);
+    // QS_JIT_THREADS_PER_SM overrides it
+    static const int env_target = [] {
+        const char* e = getenv("QS_JIT_THREADS_PER_SM");
+        return e && *e ? atoi(e) : 0;
+    }();
+    const int target = env_target > 0 ? env_target : 512;
     const int minb = threads >= target ? 1 : target / threads;
     SrcBuf g;
     g.add("// generated fused pass: n=%d K=%d L=%d R=%d stages=%d ops=%d\n", a.n, K, L, R, a.nstages, a.nops);
@@ -1492,6 +1506,15 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
     g.add("static __device__ __forceinline__ V cneg(V a) { V r; r.x = -a.x; r.y = -a.y; return r; }\n");
     g.add("static __device__ __forceinline__ V csel(bool c, V a, V b) { V r; r.x = c ? a.x : b.x; "
           "r.y = c ? a.y : b.y; return r; }\n");
+    // products with a real entry a (rmul / rfma) or an imaginary one i*b (imul / ifma)
+    g.add("static __device__ __forceinline__ V rmul(%s a, V v) { V r; r.x = a * v.x; r.y = a * v.y; return r; }\n",
+          C128 ? "double" : "float");
+    g.add("static __device__ __forceinline__ V rfma(%s a, V v, V c) { V r; r.x = %s(a, v.x, c.x); "
+          "r.y = %s(a, v.y, c.y); return r; }\n", C128 ? "double" : "float", FMA, FMA);
+    g.add("static __device__ __forceinline__ V imul(%s b, V v) { V r; r.x = -b * v.y; r.y = b * v.x; return r; }\n",
+          C128 ? "double" : "float");
+    g.add("static __device__ __forceinline__ V ifma(%s b, V v, V c) { V r; r.x = %s(-b, v.y, c.x); "
+          "r.y = %s(b, v.x, c.y); return r; }\n", C128 ? "double" : "float", FMA, FMA);
     g.add("struct __align__(16) P { V m[%d]; u64 ntiles; u64 gthr[8]; u64 gslot[%d]; u64 hibit[16]; u64 gctrl[%d]; "
           "u64 hsh[%d]; };\n", NM, E, NOPS, 4 * NOPS);
     g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
@@ -1585,22 +1608,26 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                     for (int c = 0; c < D; ++c) in[c] = var[s | pdep_c(c, mask)];
                     int outid[16];
                     for (int r = 0; r < D; ++r) {
+                        // the row's sum as a nested expression (std::string: it grows with D)
                         std::string e;
                         for (int c = 0; c < D; ++c) {
                             const int idx = op.moff + r * D + c;
                             const int cl = vclass(idx);
                             if (cl == 0) continue;
-                            char t[160];
+                            const std::string x = "v" + std::to_string(in[c]);
+                            const std::string m = "p.m[" + std::to_string(idx) + "]";
                             if (e.empty()) {
-                                if (cl == 1) snprintf(t, sizeof(t), "v%d", in[c]);
-                                else if (cl == 2) snprintf(t, sizeof(t), "cneg(v%d)", in[c]);
-                                else snprintf(t, sizeof(t), "cmul(p.m[%d], v%d)", idx, in[c]);
-                                e = t;
+                                if (cl == 1) e = x;
+                                else if (cl == 2) e = "cneg(" + x + ")";
+                                else if (cl == 4) e = "rmul(" + m + ".x, " + x + ")";
+                                else if (cl == 5) e = "imul(" + m + ".y, " + x + ")";
+                                else e = "cmul(" + m + ", " + x + ")";
                             } else {
-                                if (cl == 1) snprintf(t, sizeof(t), "cadd(%s, v%d)", e.c_str(), in[c]);
-                                else if (cl == 2) snprintf(t, sizeof(t), "cadd(%s, cneg(v%d))", e.c_str(), in[c]);
-                                else snprintf(t, sizeof(t), "cfma(p.m[%d], v%d, %s)", idx, in[c], e.c_str());
-                                e = t;
+                                if (cl == 1) e = "cadd(" + e + ", " + x + ")";
+                                else if (cl == 2) e = "cadd(" + e + ", cneg(" + x + "))";
+                                else if (cl == 4) e = "rfma(" + m + ".x, " + x + ", " + e + ")";
+                                else if (cl == 5) e = "ifma(" + m + ".y, " + x + ", " + e + ")";
+                                else e = "cfma(" + m + ", " + x + ", " + e + ")";
                             }
                         }
                         if (e.empty()) {
@@ -1609,8 +1636,12 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                             e = t;
                         }
                         outid[r] = fresh++;
-                        if (cond.empty()) g.add("    const V v%d = %s;\n", outid[r], e.c_str());
-                        else g.add("    const V v%d = c%d ? %s : v%d;\n", outid[r], o, e.c_str(), in[r]);
+                        if (cond.empty()) {
+                            g.s += "    const V v" + std::to_string(outid[r]) + " = " + e + ";\n";
+                        } else {
+                            g.s += "    const V v" + std::to_string(outid[r]) + " = c" + std::to_string(o) + " ? " + e +
+                                   " : v" + std::to_string(in[r]) + ";\n";
+                        }
                     }
                     for (int r = 0; r < D; ++r) var[s | pdep_c(r, mask)] = outid[r];
                 }
@@ -1663,6 +1694,8 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                         if (cl == 1) continue;
                         if (cl == 2) snprintf(t, sizeof(t), "cneg(v%d)", var[s]);
                         else if (cl == 0) snprintf(t, sizeof(t), "%s(0, 0)", MK);
+                        else if (cl == 4) snprintf(t, sizeof(t), "rmul(p.m[%d].x, v%d)", idx, var[s]);
+                        else if (cl == 5) snprintf(t, sizeof(t), "imul(p.m[%d].y, v%d)", idx, var[s]);
                         else snprintf(t, sizeof(t), "cmul(v%d, p.m[%d])", var[s], idx);
                     } else {
                         snprintf(t, sizeof(t), "cmul(v%d, p.m[%d + ((h%d << %d) | %du)])", var[s], int(op.moff), o,
@@ -1681,6 +1714,7 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
     }
     for (int s = 0; s < E; ++s) g.add("    vec[base | gthr | p.gslot[%d]] = v%d;\n", s, var[s]);
     g.add("  }\n}\n");
+    if (g.truncated) return false;
     out.src.swap(g.s);
     out.threads = threads;
     out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * (size_t(1) << H);
@@ -1715,6 +1749,17 @@ int launch_jit(V* vec, const RegArgs& args, int R, const V* hm, cudaStream_t st)
     return 1;
 }
 
+// Register bits per thread of generated passes: the generic kernel's (4 for
+// complex128, 5 for complex64) unless QS_JIT_REG_BITS says otherwise (4 or 5).
+inline int jit_reg_bits(int generic_r) {
+    static const int env_r = [] {
+        const char* e = getenv("QS_JIT_REG_BITS");
+        const int v = e && *e ? atoi(e) : 0;
+        return (v == 4 || v == 5) ? v : 0;
+    }();
+    return env_r ? env_r : generic_r;
+}
+
 template <typename V, int R, bool EXP, bool BIG>
 int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats, double* partials, cudaStream_t st,
                  const V* hm = nullptr) {
@@ -1722,15 +1767,27 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
     config_smem((const void*)k_fused_reg<V, R, EXP, BIG>);
     std::vector<int> rem(ps.op_count);
     for (int i = 0; i < ps.op_count; ++i) rem[i] = i;
+    const int nb = sizeof(V) == 16 ? 3 : 4;  // bank-group bits of a shared-memory phase
+    const int RJ = jit_reg_bits(R);
     while (!rem.empty()) {
-        // bank-group bits of a shared-memory phase: 8 x 16-byte or 16 x 8-byte elements
         const int next = ps.op_begin + rem.front();
-        int used = build_reg(ps, ops, rem, n, R, sizeof(V) == 16 ? 3 : 4, args);
+        if (!EXP && RJ != R && ps.k - RJ >= 5 && ps.k - RJ <= 8) {
+            // a generated pass with its own register width plans its own launch;
+            // the generic kernel re-plans the same ops when it is not ready
+            std::vector<int> saved = rem;
+            if (build_reg(ps, ops, rem, n, RJ, nb, args) > 0) {
+                int jr = launch_jit<V>(vec, args, RJ, hm, st);
+                if (jr < 0) return jr;
+                if (jr == 1) continue;
+            }
+            rem.swap(saved);
+        }
+        int used = build_reg(ps, ops, rem, n, R, nb, args);
         if (used <= 0) {
             set_error("qs_apply_fused: op %d does not fit a register tile", next);
             return QS_EINVAL;
         }
-        if (!EXP) {
+        if (!EXP && RJ == R) {
             int jr = launch_jit<V>(vec, args, R, hm, st);
             if (jr < 0) return jr;
             if (jr == 1) continue;
@@ -1915,7 +1972,7 @@ extern "C" int qs_jit_pass_source(int n, int dtype, const qs_pass* pass, const q
     QS_REQUIRE(launch_index >= 0, "negative launch index");
     int rc = validate_pass(*pass, n, ops, nops_total, mats_count);
     if (rc) return rc;
-    const int R = dtype == QS_C128 ? reg_bits<double2>() : reg_bits<float2>();
+    const int R = jit_reg_bits(dtype == QS_C128 ? reg_bits<double2>() : reg_bits<float2>());
     const int nT = pass->k - R;
     if (!(nT >= 5 && nT <= 8 && pass->nlow >= 5)) {
         set_error("qs_jit_pass_source: tile 2^%d / nlow %d is not a register tile", pass->k, pass->nlow);

@@ -75,6 +75,8 @@ struct State {
     std::deque<std::shared_ptr<Entry>> queue;
     int workers = 0;
     int pending = 0;
+    int running = 0;
+    bool stopping = false;
     std::string last_log;
     std::atomic<int> mode{-1};
     std::atomic<int64_t> compiled{0}, failed{0}, jit_launches{0}, fallback_launches{0}, hits{0};
@@ -182,12 +184,30 @@ void worker_loop() {
         std::shared_ptr<Entry> e;
         {
             std::unique_lock<std::mutex> lock(s.mu);
-            s.cv.wait(lock, [&] { return !s.queue.empty(); });
+            s.cv.wait(lock, [&] { return !s.queue.empty() || s.stopping; });
+            if (s.stopping) return;
             e = s.queue.front();
             s.queue.pop_front();
+            ++s.running;
         }
         compile_entry(s, *e);
+        std::lock_guard<std::mutex> lock(s.mu);
+        --s.running;
+        s.cv.notify_all();
     }
+}
+
+// At process exit: drop queued work and let running compilations finish, so
+// no worker is inside NVRTC while the process tears its libraries down.
+void shutdown_workers() {
+    State& s = S();
+    std::unique_lock<std::mutex> lock(s.mu);
+    s.stopping = true;
+    for (auto& e : s.queue) e->state = 2;
+    s.pending -= int(s.queue.size());
+    s.queue.clear();
+    s.cv.notify_all();
+    s.cv.wait_for(lock, std::chrono::seconds(120), [&] { return s.running == 0; });
 }
 
 void start_workers(State& s) {  // with s.mu held
@@ -197,6 +217,7 @@ void start_workers(State& s) {  // with s.mu held
     if (n > 16) n = 16;
     for (int i = 0; i < n; ++i) std::thread(worker_loop).detach();
     s.workers = n;
+    std::atexit(shutdown_workers);
 }
 
 // Loaded function of a ready entry on the current device (with s.mu held).

@@ -210,7 +210,46 @@ def _to_op(bits: Tuple[int, ...], u: np.ndarray) -> Op:
     return Op(kind, tuple(bits), (), u)
 
 
-def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bits: int = 4) -> List[Op]:
+def matrix_instr(u: np.ndarray) -> float:
+    """Floating-point instructions per amplitude the generated pass code
+    spends on a dense matrix: per output row, each entry that is neither 0
+    nor +-1 costs 4 (complex) or 2 (real or imaginary: two products), each
+    +-1 entry a complex add (2; none when it comes first), averaged over rows.
+    Rows of an identity block cost nothing."""
+    u = np.asarray(u)
+    nz = u != 0
+    unit = (u == 1) | (u == -1)
+    cheap = nz & ~unit & ((u.imag == 0) | (u.real == 0))
+    general = nz & ~unit & ~cheap
+    per_row = 4 * general.sum(axis=1) + 2 * cheap.sum(axis=1) + 2 * unit.sum(axis=1)
+    first_unit = np.array([bool(unit[r, np.flatnonzero(nz[r])[0]]) if nz[r].any() else False
+                           for r in range(u.shape[0])])
+    per_row = per_row - 2 * first_unit
+    return float(per_row.mean())
+
+
+def op_instr(op: Op) -> float:
+    """``matrix_instr`` of an op (controls folded in); diagonals: 4 per
+    entry that is not 1 (2 when real or imaginary), averaged; plain
+    exchanges cost nothing (the generated code renames registers)."""
+    if op.kind == "diag":
+        d = np.asarray(op.mat).ravel()
+        c = np.where(d == 1, 0, np.where((d.imag == 0) | (d.real == 0), 2, 4))
+        return float(c.mean()) * 0.5 ** len(op.cbits)
+    if op.kind in ("antidiag", "swap") and _unit_exchange(op):
+        return 0.0
+    return matrix_instr(op.dense()) * 0.5 ** len(op.cbits)
+
+
+def _unit_exchange(op: Op) -> bool:
+    m = op.mat
+    if op.kind == "antidiag":
+        return m[0, 1] == 1 and m[1, 0] == 1
+    return _unit_swap(op)
+
+
+def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bits: int = 4,
+              cost_aware: bool = True) -> List[Op]:
     """Multiply runs of ops that act on at most `max_bits` tile-resident bits
     into single ops (gate fusion at the matrix level).  Diagonal ops (phases,
     Rz, Rzz, CZ, ...) also merge among themselves into diagonal blocks of up to
@@ -221,9 +260,14 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bi
     that touches several blocks closes them (emits them) first, and an op that
     cannot be merged (bits outside the tile, too many bits, tagged for
     gradients) closes the blocks it touches and is emitted as is.  Order is
-    therefore preserved between every pair of ops that share a bit."""
+    therefore preserved between every pair of ops that share a bit.
+
+    With `cost_aware`, a dense merge happens only when the product costs no
+    more floating-point instructions (``matrix_instr``) than the blocks and
+    the op apart: a plain exchange, or a real 1-qubit gate such as H or Ry,
+    can be cheaper on its own than inside a general 4 x 4 product."""
     out: List[Op] = []
-    blocks: List[list] = []  # [bits tuple, matrix, [source ops], all diagonal]
+    blocks: List[list] = []  # [bits tuple, matrix, [source ops], all diagonal, instr]
 
     def close(b):
         blocks.remove(b)
@@ -245,6 +289,15 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bi
         elif free and union <= tile and len(union) <= max_bits:
             as_diag = diag and all(b[3] for b in hit)
         else:
+            as_diag = None
+        merged = None
+        if as_diag is not None:
+            merged = _merge_blocks(hit, op)
+            if cost_aware and not as_diag:
+                apart = sum(_block_instr(b) for b in hit) + op_instr(op)
+                if matrix_instr(merged[1]) > apart:
+                    merged = None
+        if merged is None:
             for b in hit:
                 close(b)
             if free and ((diag and len(S) <= max_diag_bits) or (S <= tile and len(S) <= max_bits)):
@@ -253,29 +306,39 @@ def merge_ops(ops: Sequence[Op], tile: frozenset, max_bits: int = 2, max_diag_bi
             else:
                 out.append(op)
             continue
-        # merge the hit blocks (disjoint, commuting) and the op into one block
-        bits: Tuple[int, ...] = ()
-        u = None  # the first factor is taken as is (no product with an identity)
-        srcs: List[Op] = []
         for b in hit:
-            if u is None:
-                bits, u = b[0], b[1]
-            else:
-                nb = bits + tuple(x for x in b[0] if x not in bits)
-                u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
-                bits = nb
-            srcs += b[2]
             blocks.remove(b)
-        ob, ou = _full_matrix(op)
-        if u is None:
-            nb, u = ob, ou
-        else:
-            nb = bits + tuple(x for x in ob if x not in bits)
-            u = _embed(ou, ob, nb) @ _embed(u, bits, nb)
-        blocks.append([nb, u, srcs + [op], as_diag])
+        nb, u, srcs = merged
+        blocks.append([nb, u, srcs, as_diag])
     for b in list(blocks):
         close(b)
     return out
+
+
+def _block_instr(b) -> float:
+    """Instructions of an open block as it would be emitted."""
+    return op_instr(b[2][0]) if len(b[2]) == 1 else matrix_instr(b[1])
+
+
+def _merge_blocks(hit, op):
+    """(bits, matrix, source ops) of the product of the hit blocks (disjoint,
+    commuting) and the op."""
+    bits: Tuple[int, ...] = ()
+    u = None  # the first factor is taken as is (no product with an identity)
+    srcs: List[Op] = []
+    for b in hit:
+        if u is None:
+            bits, u = b[0], b[1]
+        else:
+            nb = bits + tuple(x for x in b[0] if x not in bits)
+            u = _embed(b[1], b[0], nb) @ _embed(u, bits, nb)
+            bits = nb
+        srcs += b[2]
+    ob, ou = _full_matrix(op)
+    if u is None:
+        return ob, ou, srcs + [op]
+    nb = bits + tuple(x for x in ob if x not in bits)
+    return nb, _embed(ou, ob, nb) @ _embed(u, bits, nb), srcs + [op]
 
 
 def op_entries(op: Op) -> int:

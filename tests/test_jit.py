@@ -62,6 +62,22 @@ def test_generator_emits_every_register_launch_and_nvrtc_compiles_one():
     assert nb.value > 1000
 
 
+@pytest.mark.parametrize("esize", [16, 8])
+def test_longest_generated_sources_compile(esize):
+    """3-bit merged blocks give the longest row expressions; the launches
+    with the most code of such a plan must compile."""
+    from quict_b200 import _native as N
+    from quict_b200.simulation.autotune import Knobs
+    lib = N.load()
+    srcs = sorted(_plan_sources(20, esize, gates=400, knobs=Knobs(12 if esize == 16 else 13, 5, 3)), key=len)
+    for src in srcs[-2:]:
+        nb = C.c_int64(0)
+        rc = lib.qs_jit_compile_check(src.encode(), C.byref(nb))
+        if rc == N.QS_ENOTSUP:
+            pytest.skip("NVRTC is not available here")
+        assert rc == 0, lib.qs_jit_last_log()
+
+
 def test_jit_mode_and_stats_entry_points():
     from quict_b200 import _native as N
     prev = N.jit_set_mode(N.QS_JIT_OFF)
@@ -92,17 +108,26 @@ def test_compiled_passes_vs_oracle_for_every_tuner_knob(cuda_ok, jit_sync, preci
     N = jit_sync
     esize = 16 if precision == "double" else 8
     tol = 1e-12 if precision == "double" else 1e-5
-    before = N.jit_stats()["compiled_launches"]
+    cases = []
     for n in (14, 17):
         gl = _every_placement_circuit(n, seed=200 + n)
-        ref = osv.run(oracle_gates(build_circuit(gl, n)), n)
-        for kn in candidates(esize, n):
-            s = StateVectorSimulator("GPU", precision, tile_bits=kn.tile_bits, low_bits=kn.low_bits,
-                                     merge_bits=kn.merge_bits)
-            v = s.run(build_circuit(gl, n, precision)).get()
-            err = float(np.max(np.abs(v - ref)))
-            assert err < tol, (n, kn, err)
-    assert N.jit_stats()["compiled_launches"] > before, N.load().qs_jit_last_log()
+        cases.append((n, gl, osv.run(oracle_gates(build_circuit(gl, n)), n)))
+    # first round in ASYNC mode: generic kernels run while the pool compiles
+    # every pass shape in parallel; the second round (SYNC) runs them compiled
+    for mode in (N.QS_JIT_ASYNC, N.QS_JIT_SYNC):
+        N.jit_set_mode(mode)
+        before = N.jit_stats()
+        for n, gl, ref in cases:
+            for kn in candidates(esize, n):
+                s = StateVectorSimulator("GPU", precision, tile_bits=kn.tile_bits, low_bits=kn.low_bits,
+                                         merge_bits=kn.merge_bits)
+                v = s.run(build_circuit(gl, n, precision)).get()
+                err = float(np.max(np.abs(v - ref)))
+                assert err < tol, (mode, n, kn, err)
+        N.jit_wait(900)
+    after = N.jit_stats()
+    assert after["compiled_launches"] > before["compiled_launches"], N.load().qs_jit_last_log()
+    assert after["failed"] == before["failed"], N.load().qs_jit_last_log()
 
 
 @pytest.mark.gpu
@@ -118,6 +143,9 @@ def test_compiled_passes_match_generic_kernels_at_26_qubits(cuda_ok, precision):
     prev = N.jit_set_mode(N.QS_JIT_OFF)
     try:
         a = StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1)).tensor
+        N.jit_set_mode(N.QS_JIT_ASYNC)  # queue every pass shape for the compile pool
+        StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1))
+        N.jit_wait(900)
         N.jit_set_mode(N.QS_JIT_SYNC)
         before = N.jit_stats()["compiled_launches"]
         b = StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1)).tensor
