@@ -326,6 +326,32 @@ def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
             "state_bytes": (1 << n) * (16 if precision == "double" else 8)}
 
 
+def c64_error(n, local):
+    """complex64 against complex128 on the config-1 circuit at n qubits (both
+    run by this GPU; the complex128 path is checked against the FP64 oracle
+    and the per-gate kernels by the parity tests): max |amplitude error| and
+    max error of <Z> on a spread of qubits (FP64 P(0) reductions)."""
+    import numpy as np
+    import torch
+    from quict_b200.simulation import StateVectorSimulator
+    from quict_b200.workloads import config1_circuit
+    a = StateVectorSimulator("GPU", "double", gpu_device_id=local)
+    va = a.run(config1_circuit(n, N_GATES, SEED)).tensor
+    b = StateVectorSimulator("GPU", "single", gpu_device_id=local)
+    vb = b.run(config1_circuit(n, N_GATES, SEED)).tensor
+    amp = 0.0
+    for i in range(0, va.numel(), 1 << 27):
+        amp = max(amp, float((va[i:i + (1 << 27)] - vb[i:i + (1 << 27)].to(torch.complex128)).abs().max()))
+    bits = sorted({0, 1, 4, n // 2, n - 2, n - 1})
+    za = np.array([2 * a.engine.prob0(va, n, q) - 1 for q in bits])
+    zb = np.array([2 * b.engine.prob0(vb, n, q) - 1 for q in bits])
+    out = {"max_abs_amp_err_vs_c128": amp, "max_abs_z_expectation_err_vs_c128": float(np.max(np.abs(za - zb))),
+           "z_vector_bits": bits}
+    del a, b, va, vb
+    torch.cuda.empty_cache()
+    return out
+
+
 def grad_bench(ws, rank, local, batch=1024):
     """Config 3: HEA 16q x 8 layers, 256 params, batch 1024 (split over ranks),
     H = sum ZZ + 0.5 sum X.  Adjoint gradient (c64, c128) vs the same GPU's
@@ -690,7 +716,11 @@ def run_ours(args, ws, rank, local):
     del sim, vec
     torch.cuda.empty_cache()
     if not args.no_extra:
-        line["c64"] = [sv_rate(30, "single", local, ws), sv_rate(32, "single", local, ws)]
+        line["c64"] = []
+        for nq in (30, 32):
+            row = sv_rate(nq, "single", local, ws)
+            row.update(c64_error(nq, local))
+            line["c64"].append(row)
     if not args.no_extra:
         line["configs_0_2"] = small_configs_bench(ws, local)
     if not args.no_grad:

@@ -182,6 +182,14 @@ int qs_apply_fused_ex(void* vec, int n, int dtype, const qs_pass* passes, int np
                       const qs_op* ops, int64_t nops_total, const void* mats_dev,
                       const void* mats_host, int64_t mats_count, void* stream);
 
+/* qs_adjoint_pair with the matrix table also in HOST memory (as
+ * qs_apply_fused_ex): pair passes then run as generated kernels when the
+ * JIT mode allows it, with per-instance tables staged in shared memory. */
+int qs_adjoint_pair_ex(void* psilam, int n, int dtype, const qs_pass* passes, int npasses,
+                       const qs_op* ops, int64_t nops_total, const void* mats_dev,
+                       const void* mats_host, int64_t mats_count, double* partials_dev,
+                       int64_t partials_count, void* stream);
+
 /* ---- run-time compiled passes ------------------------------------------------ */
 #define QS_JIT_OFF   0    /* generic fused kernels only                             */
 #define QS_JIT_ASYNC 1    /* compile on host threads; generic kernels meanwhile (default;
@@ -196,6 +204,10 @@ int qs_jit_wait(double timeout_s);
  * launches of compiled kernels, launches that ran the generic kernel while a
  * compilation was pending, total compile milliseconds, cache hits. */
 int qs_jit_stats(int64_t* out, int n);
+/* Drop queued compilations and wait for the running ones to finish (call
+ * before the process exits while compilations may be running; passes not yet
+ * compiled keep running on the generic kernels). */
+int qs_jit_shutdown(void);
 /* Log of the last failed compilation or load ("" if none). */
 const char* qs_jit_last_log(void);
 /* Compile `src` with NVRTC only (no device needed); *cubin_bytes <- size. */

@@ -6,6 +6,7 @@ raises ``NativeLibraryError``.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 
@@ -108,6 +109,9 @@ SIGNATURES = {
     "qs_histogram": (_i, [_vp, _i64, _vp, _i64, _vp]),
     "qs_sample_noalloc": (_i, [_vp, _i, _i, _i, _vp, _i64, _i, _vp, _vp]),
     "qs_apply_fused_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp]),
+    "qs_adjoint_pair_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp,
+                                _i64, _vp]),
+    "qs_jit_shutdown": (_i, []),
     "qs_jit_set_mode": (_i, [_i]),
     "qs_jit_wait": (_i, [_d]),
     "qs_jit_stats": (_i, [C.POINTER(C.c_int64), _i]),
@@ -138,6 +142,8 @@ def load() -> C.CDLL:
         f.restype = res
         f.argtypes = args
     _lib = lib
+    # no pass compilation may still run while the interpreter shuts down
+    atexit.register(lib.qs_jit_shutdown)
     return lib
 
 

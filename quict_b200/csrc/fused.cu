@@ -26,8 +26,11 @@
 #include <array>
 #include <cstdarg>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -1423,28 +1426,39 @@ std::string thread_xor_expr(const uint32_t* img, int nT) {
 }
 
 template <typename V>
-bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
+bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_source = true) {
     constexpr bool C128 = sizeof(V) == 16;
     const int E = 1 << R, nT = a.nT, K = a.K, L = a.L, H = a.H;
-    const int threads = 1 << nT;
+    const int threads = 1 << nT, nwarps = threads / 32;
     const int NM = a.nmats > 0 ? a.nmats : 1;
     const int NOPS = a.nops > 0 ? a.nops : 1;
-    // ---- parameter block: V m[NM]; u64 ntiles, gthr[8], gslot[E], hibit[16], gctrl[NOPS], hsh[4 NOPS]
-    const size_t off_u64 = sizeof(V) * size_t(NM);
-    const size_t o_ntiles = off_u64, o_gthr = o_ntiles + 8, o_gslot = o_gthr + 64, o_hibit = o_gslot + 8 * E,
-                 o_gctrl = o_hibit + 128, o_hsh = o_gctrl + 8 * size_t(NOPS);
-    size_t bytes = o_hsh + 32 * size_t(NOPS);
+    const int NEXP = a.nexp > 0 ? a.nexp : 1;
+    const bool batched = a.batched != 0;
+    // ---- parameter block (all fields 8-byte aligned, V first):
+    //   V m[NM]; u64 ntiles, gthr[8], gslot[E], hibit[16], gctrl[NOPS], hsh[4 NOPS],
+    //   mgoff[NOPS], mstride[NOPS], eslot[NEXP], misc[2]; u32 pe[NM]
+    // m holds every op's matrix in slot order; for a batched pass the ops with
+    // per-instance tables (stride != 0) are staged into shared memory per
+    // instance instead: pe[g] = (op << 16) | offset within the instance block
+    const size_t o_ntiles = sizeof(V) * size_t(NM), o_gthr = o_ntiles + 8, o_gslot = o_gthr + 64,
+                 o_hibit = o_gslot + 8 * size_t(E), o_gctrl = o_hibit + 128, o_hsh = o_gctrl + 8 * size_t(NOPS),
+                 o_mgoff = o_hsh + 32 * size_t(NOPS), o_mstride = o_mgoff + 8 * size_t(NOPS),
+                 o_eslot = o_mstride + 8 * size_t(NOPS), o_misc = o_eslot + 8 * size_t(NEXP), o_pe = o_misc + 16;
+    size_t bytes = o_pe + (batched ? 4 * size_t(NM) : 0);
     bytes = (bytes + 15) & ~size_t(15);
     if (bytes > kJitMaxParamBytes) return false;
     out.params.assign(bytes / 8, 0);
     unsigned char* pb = reinterpret_cast<unsigned char*>(out.params.data());
     auto put64 = [&](size_t off, uint64_t v) { memcpy(pb + off, &v, 8); };
-    // matrices in slot order, exactly as the generic kernel stages them
     V* pm = reinterpret_cast<V*>(pb);
+    std::vector<char> strided(size_t(NOPS), 0);
     for (int o = 0; o < a.nops; ++o) {
         const KCopy& c = a.cp[o];
         const int D = 1 << c.m;
         const int cnt = c.diag ? D : D * D;
+        strided[o] = batched && c.stride != 0;
+        put64(o_mgoff + 8 * size_t(o), uint64_t(c.goff));
+        put64(o_mstride + 8 * size_t(o), uint64_t(c.stride));
         for (int e = 0; e < cnt; ++e) {
             const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
             int sr = 0, sc = 0;
@@ -1452,9 +1466,24 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                 sr |= ((kr >> i) & 1) << c.perm[i];
                 sc |= ((kc >> i) & 1) << c.perm[i];
             }
-            pm[c.soff + e] = hm[c.goff + (c.diag ? sr : sr * D + sc)];
+            const int src = c.diag ? sr : sr * D + sc;
+            if (strided[o]) {  // bit 31 marks a staged entry
+                const uint32_t v = (1u << 31) | (uint32_t(o) << 16) | uint32_t(src);
+                memcpy(pb + o_pe + 4 * size_t(c.soff + e), &v, 4);
+            } else {
+                pm[c.soff + e] = hm[c.goff + src];
+            }
         }
     }
+    if (a.nops > 32767) return false;
+    // tile position of the psi/lam pair bit (adjoint pair passes)
+    int pair_tile = -1;
+    for (int b = 0; b < 64 && a.pairmask; ++b)
+        if ((a.pairmask >> b) & 1) {
+            if (b < L) pair_tile = b;
+            for (int t = 0; t < H; ++t)
+                if (a.hi[t] == b) pair_tile = L + t;
+        }
     auto gbit = [&](int b) -> uint64_t { return uint64_t(1) << (b < L ? b : a.hi[b - L]); };
     const KStage& SL = a.st[a.nstages - 1];
     put64(o_ntiles, uint64_t(1) << (a.n - K));
@@ -1471,10 +1500,13 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
         for (int q = 0; q < a.ops[o].nh; ++q)
             put64(o_hsh + 32 * o + 8 * q, a.ops[o].hsrc[q] >= 64 ? uint64_t(a.ops[o].hsrc[q] - 64) : 0);
     }
-    // value class of a parameter-block entry: 0, 1, -1, general (3), real (4),
-    // imaginary (5); a real or imaginary entry multiplies with two products
-    // instead of four
-    auto vclass = [&](int idx) -> int {
+    for (int e = 0; e < a.nexp; ++e) put64(o_eslot + 8 * e, uint64_t(a.eslot[e]));
+    put64(o_misc, ~a.pairmask);
+    put64(o_misc + 8, uint64_t(a.inst_shift));
+    // value class of a matrix entry: 0, 1, -1, general (3), real (4), imaginary
+    // (5); entries of per-instance tables are general
+    auto vclass = [&](int o, int idx) -> int {
+        if (strided[o]) return 3;
         const V v = pm[idx];
         if (v.y == 0) {
             if (v.x == 0) return 0;
@@ -1484,7 +1516,17 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
         }
         return v.x == 0 ? 5 : 3;
     };
+    auto mref = [&](int o, int idx) -> std::string {
+        return (strided[o] ? "msm[" : "p.m[") + std::to_string(idx) + "]";
+    };
+    const unsigned hoff_n = (1u << H) < 2u ? 2u : (1u << H);  // a 16-byte multiple
+    out.threads = threads;
+    out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * size_t(hoff_n) +
+               (a.nexp > 0 ? sizeof(double2) * size_t(nwarps) * size_t(a.nexp) : 0) +
+               (batched ? sizeof(V) * size_t(NM) : 0);
+    if (!with_source) return true;
     const char* VT = C128 ? "double2" : "float2";
+    const char* ST = C128 ? "double" : "float";
     const char* MK = C128 ? "make_double2" : "make_float2";
     const char* FMA = C128 ? "__fma_rn" : "__fmaf_rn";
     // resident threads per SM the register budget is sized for (launch bounds);
@@ -1496,8 +1538,9 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
     const int target = env_target > 0 ? env_target : 512;
     const int minb = threads >= target ? 1 : target / threads;
     SrcBuf g;
-    g.add("// generated fused pass: n=%d K=%d L=%d R=%d stages=%d ops=%d\n", a.n, K, L, R, a.nstages, a.nops);
-    g.add("typedef unsigned long long u64;\ntypedef unsigned int u32;\ntypedef %s V;\n", VT);
+    g.add("// generated fused pass: n=%d K=%d L=%d R=%d stages=%d ops=%d expect=%d batched=%d\n", a.n, K, L, R,
+          a.nstages, a.nops, a.nexp, int(batched));
+    g.add("typedef unsigned long long u64;\ntypedef unsigned int u32;\ntypedef %s V;\ntypedef %s S;\n", VT, ST);
     g.add("static __device__ __forceinline__ V cmul(V a, V b) { V r; r.x = a.x * b.x - a.y * b.y; "
           "r.y = a.x * b.y + a.y * b.x; return r; }\n");
     g.add("static __device__ __forceinline__ V cfma(V a, V b, V c) { V r; r.x = %s(a.x, b.x, %s(-a.y, b.y, c.x)); "
@@ -1507,27 +1550,27 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
     g.add("static __device__ __forceinline__ V csel(bool c, V a, V b) { V r; r.x = c ? a.x : b.x; "
           "r.y = c ? a.y : b.y; return r; }\n");
     // products with a real entry a (rmul / rfma) or an imaginary one i*b (imul / ifma)
-    g.add("static __device__ __forceinline__ V rmul(%s a, V v) { V r; r.x = a * v.x; r.y = a * v.y; return r; }\n",
-          C128 ? "double" : "float");
-    g.add("static __device__ __forceinline__ V rfma(%s a, V v, V c) { V r; r.x = %s(a, v.x, c.x); "
-          "r.y = %s(a, v.y, c.y); return r; }\n", C128 ? "double" : "float", FMA, FMA);
-    g.add("static __device__ __forceinline__ V imul(%s b, V v) { V r; r.x = -b * v.y; r.y = b * v.x; return r; }\n",
-          C128 ? "double" : "float");
-    g.add("static __device__ __forceinline__ V ifma(%s b, V v, V c) { V r; r.x = %s(-b, v.y, c.x); "
-          "r.y = %s(b, v.x, c.y); return r; }\n", C128 ? "double" : "float", FMA, FMA);
+    g.add("static __device__ __forceinline__ V rmul(S a, V v) { V r; r.x = a * v.x; r.y = a * v.y; return r; }\n");
+    g.add("static __device__ __forceinline__ V rfma(S a, V v, V c) { V r; r.x = %s(a, v.x, c.x); "
+          "r.y = %s(a, v.y, c.y); return r; }\n", FMA, FMA);
+    g.add("static __device__ __forceinline__ V imul(S b, V v) { V r; r.x = -b * v.y; r.y = b * v.x; return r; }\n");
+    g.add("static __device__ __forceinline__ V ifma(S b, V v, V c) { V r; r.x = %s(-b, v.y, c.x); "
+          "r.y = %s(b, v.x, c.y); return r; }\n", FMA, FMA);
     g.add("struct __align__(16) P { V m[%d]; u64 ntiles; u64 gthr[8]; u64 gslot[%d]; u64 hibit[16]; u64 gctrl[%d]; "
-          "u64 hsh[%d]; };\n", NM, E, NOPS, 4 * NOPS);
+          "u64 hsh[%d]; u64 mgoff[%d]; u64 mstride[%d]; u64 eslot[%d]; u64 misc[2];%s };\n", NM, E, NOPS, 4 * NOPS,
+          NOPS, NOPS, NEXP, batched ? (" u32 pe[" + std::to_string(NM) + "];").c_str() : "");
     g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
-          "const __grid_constant__ P p) {\n", threads, minb);
+          "const __grid_constant__ P p, const V* __restrict__ mats, double* __restrict__ partials) {\n", threads, minb);
     g.add("  extern __shared__ __align__(16) unsigned char smem_raw[];\n");
     g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", 1u << K);
     g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
+    g.add("  double2* const ered = reinterpret_cast<double2*>(hoff + %du);\n", hoff_n);
+    g.add("  V* const msm = reinterpret_cast<V*>(ered + %d);\n", a.nexp > 0 ? nwarps * a.nexp : 0);
     g.add("  const u32 tid = threadIdx.x;\n");
     g.add("  for (u32 j = tid; j < %du; j += %du) { u64 o = 0;\n", 1u << H, threads);
     g.add("#pragma unroll\n    for (int t = 0; t < %d; ++t) if ((j >> t) & 1u) o |= p.hibit[t];\n    hoff[j] = o; }\n", H);
     g.add("  u64 gthr = 0;\n");
     for (int i = 0; i < nT; ++i) g.add("  if ((tid >> %d) & 1u) gthr |= p.gthr[%d];\n", i, i);
-    // per-stage thread images
     for (int si = 0; si < a.nstages; ++si) {
         const KStage& S = a.st[si];
         uint32_t rt[8], wt[8], tb[8];
@@ -1540,11 +1583,20 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
         if (si > 0) g.add("  const u32 WR%d = %s;\n", si, thread_xor_expr(wt, nT).c_str());
         g.add("  const u32 TH%d = %s;\n", si, thread_xor_expr(tb, nT).c_str());
     }
-    g.add("  __syncthreads();\n");
-    g.add("  const u64 ntiles = p.ntiles;\n  const u64 tstep = gridDim.x;\n  u64 tile = blockIdx.x;\n");
+    g.add("  const u64 ntiles = p.ntiles;\n");
     g.add("  auto tile_base = [&](u64 t) -> u64 { u64 b = t << %d;\n", L);
     g.add("#pragma unroll\n    for (int i = 0; i < %d; ++i) { const u64 lo = p.hibit[i] - 1ull; "
           "b = ((b & ~lo) << 1) | (b & lo); }\n    return b; };\n", H);
+    if (batched) {
+        // per-instance tables: contiguous runs of tiles per CTA, so that a CTA
+        // restages its instance's matrices once per instance
+        g.add("  const u64 chunk = (ntiles + gridDim.x - 1) / gridDim.x;\n");
+        g.add("  u64 tile = u64(blockIdx.x) * chunk;\n  const u64 tend = tile + chunk < ntiles ? tile + chunk : ntiles;\n");
+        g.add("  const u64 tstep = 1;\n  u64 staged = ~0ull;\n");
+    } else {
+        g.add("  u64 tile = blockIdx.x;\n  const u64 tend = ntiles;\n  const u64 tstep = gridDim.x;\n");
+    }
+    g.add("  __syncthreads();\n");
     const int EPC = 16 / int(sizeof(V));
     g.add("  auto prefetch = [&](V* dst, u64 base) {\n");
     g.add("    for (u32 c = tid; c < %du; c += %du) { const u32 e = c * %du;\n", (1u << K) / EPC, threads, EPC);
@@ -1552,19 +1604,65 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
     g.add("      asm volatile(\"cp.async.cg.shared.global [%%0], [%%1], 16;\\n\" :: \"r\"(sa), "
           "\"l\"(vec + (base | hoff[e >> %d] | (e & %du))) : \"memory\"); }\n", L, (1u << L) - 1u);
     g.add("    asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\"); };\n");
-    g.add("  if (tile < ntiles) prefetch(b0, tile_base(tile));\n");
-    g.add("  for (u32 it = 0; tile < ntiles; ++it, tile += tstep) {\n");
+    g.add("  if (tile < tend) prefetch(b0, tile_base(tile));\n");
+    g.add("  for (u32 it = 0; tile < tend; ++it, tile += tstep) {\n");
     g.add("    V* const cur = (it & 1u) ? b1 : b0;\n    const u64 base = tile_base(tile);\n");
     g.add("    asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n    __syncthreads();\n");
-    g.add("    if (tile + tstep < ntiles) prefetch((it & 1u) ? b0 : b1, tile_base(tile + tstep));\n");
+    g.add("    if (tile + tstep < tend) prefetch((it & 1u) ? b0 : b1, tile_base(tile + tstep));\n");
+    if (batched) {
+        g.add("    { const u64 inst = (base & p.misc[0]) >> p.misc[1];\n");
+        g.add("      if (inst != staged) {\n");
+        g.add("        for (u32 q = tid; q < %du; q += %du) { const u32 v = p.pe[q];\n", unsigned(a.nmats), threads);
+        g.add("          if (v >> 31) { const u32 o = (v >> 16) & 0x7fffu; "
+              "msm[q] = mats[p.mgoff[o] + inst * p.mstride[o] + (v & 0xffffu)]; } }\n");
+        g.add("        staged = inst;\n        __syncthreads();\n      } }\n");
+    }
     // ---- body
     int fresh = 0;
     std::vector<int> var(E);  // slot -> SSA value id
+    auto vname = [&](int id) { return "v" + std::to_string(id); };
     auto slot_addr = [&](const uint16_t* img, int s) {
         uint32_t c = 0;
         for (int j = 0; j < R; ++j)
             if ((s >> j) & 1) c ^= img[j];
         return c;
+    };
+    // the sum over the nonzero entries of one row of a (slot-order) matrix
+    auto row_expr = [&](int o, int base_idx, int D, const int* in) -> std::string {
+        std::string e;
+        for (int c = 0; c < D; ++c) {
+            const int idx = base_idx + c;
+            const int cl = vclass(o, idx);
+            if (cl == 0) continue;
+            const std::string x = vname(in[c]);
+            const std::string m = mref(o, idx);
+            if (e.empty()) {
+                if (cl == 1) e = x;
+                else if (cl == 2) e = "cneg(" + x + ")";
+                else if (cl == 4) e = "rmul(" + m + ".x, " + x + ")";
+                else if (cl == 5) e = "imul(" + m + ".y, " + x + ")";
+                else e = "cmul(" + m + ", " + x + ")";
+            } else {
+                if (cl == 1) e = "cadd(" + e + ", " + x + ")";
+                else if (cl == 2) e = "cadd(" + e + ", cneg(" + x + "))";
+                else if (cl == 4) e = "rfma(" + m + ".x, " + x + ", " + e + ")";
+                else if (cl == 5) e = "ifma(" + m + ".y, " + x + ", " + e + ")";
+                else e = "cfma(" + m + ", " + x + ", " + e + ")";
+            }
+        }
+        if (e.empty()) e = std::string(MK) + "(0, 0)";
+        return e;
+    };
+    // thread-dependent / outside-tile index bits of a diagonal (h), as an expression
+    auto h_expr = [&](const KOp& op, int o, int si) -> std::string {
+        std::string h;
+        for (int q = 0; q < op.nh; ++q) {
+            const int src = op.hsrc[q];
+            const std::string t = src < 64 ? "((TH" + std::to_string(si) + " >> " + std::to_string(src) + ") & 1u)"
+                                            : "u32((base >> p.hsh[" + std::to_string(4 * o + q) + "]) & 1ull)";
+            h = h.empty() ? t : "((" + h + ") << 1) | " + t;
+        }
+        return h;
     };
     for (int s = 0; s < E; ++s) {
         var[s] = fresh++;
@@ -1584,64 +1682,28 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
         for (int o = S.op_begin; o < S.op_begin + S.op_count; ++o) {
             const KOp& op = a.ops[o];
             std::string cond;
-            if (op.gctrl) {
-                char t[96];
-                snprintf(t, sizeof(t), "((base & p.gctrl[%d]) == p.gctrl[%d])", o, o);
-                cond = t;
-            }
+            if (op.gctrl) cond = "((base & p.gctrl[" + std::to_string(o) + "]) == p.gctrl[" + std::to_string(o) + "])";
             if (op.tctrl) {
-                char t[96];
-                snprintf(t, sizeof(t), "%s((TH%d & %uu) == %uu)", cond.empty() ? "" : " && ", si, unsigned(op.tctrl),
-                         unsigned(op.tctrl));
-                cond += t;
+                const std::string tc = std::to_string(unsigned(op.tctrl)) + "u";
+                cond += (cond.empty() ? "" : " && ") + std::string("((TH") + std::to_string(si) + " & " + tc +
+                        ") == " + tc + ")";
             }
             const int scm = op.scm;
             auto ctrl_ok = [&](int s) { return (s & scm) == scm; };
+            if (!cond.empty() && op.code != QS_OP_EXPECT) g.add("    const bool c%d = %s;\n", o, cond.c_str());
             if (op.code == QS_OP_MAT) {
                 const int mask = op.mask, M = popc_c(mask), D = 1 << M;
-                std::vector<std::pair<int, int>> groups;  // (s, first new id)
-                g.add("    // op %d: dense on slot mask %d%s\n", o, mask, cond.empty() ? "" : " (controlled)");
-                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
+                g.add("    // op %d: dense on slot mask %d\n", o, mask);
                 for (int s = 0; s < E; ++s) {
                     if ((s & mask) || !ctrl_ok(s)) continue;
-                    int in[16];
+                    int in[16], outid[16];
                     for (int c = 0; c < D; ++c) in[c] = var[s | pdep_c(c, mask)];
-                    int outid[16];
                     for (int r = 0; r < D; ++r) {
-                        // the row's sum as a nested expression (std::string: it grows with D)
-                        std::string e;
-                        for (int c = 0; c < D; ++c) {
-                            const int idx = op.moff + r * D + c;
-                            const int cl = vclass(idx);
-                            if (cl == 0) continue;
-                            const std::string x = "v" + std::to_string(in[c]);
-                            const std::string m = "p.m[" + std::to_string(idx) + "]";
-                            if (e.empty()) {
-                                if (cl == 1) e = x;
-                                else if (cl == 2) e = "cneg(" + x + ")";
-                                else if (cl == 4) e = "rmul(" + m + ".x, " + x + ")";
-                                else if (cl == 5) e = "imul(" + m + ".y, " + x + ")";
-                                else e = "cmul(" + m + ", " + x + ")";
-                            } else {
-                                if (cl == 1) e = "cadd(" + e + ", " + x + ")";
-                                else if (cl == 2) e = "cadd(" + e + ", cneg(" + x + "))";
-                                else if (cl == 4) e = "rfma(" + m + ".x, " + x + ", " + e + ")";
-                                else if (cl == 5) e = "ifma(" + m + ".y, " + x + ", " + e + ")";
-                                else e = "cfma(" + m + ", " + x + ", " + e + ")";
-                            }
-                        }
-                        if (e.empty()) {
-                            char t[64];
-                            snprintf(t, sizeof(t), "%s(0, 0)", MK);
-                            e = t;
-                        }
+                        const std::string e = row_expr(o, op.moff + r * D, D, in);
                         outid[r] = fresh++;
-                        if (cond.empty()) {
-                            g.s += "    const V v" + std::to_string(outid[r]) + " = " + e + ";\n";
-                        } else {
-                            g.s += "    const V v" + std::to_string(outid[r]) + " = c" + std::to_string(o) + " ? " + e +
-                                   " : v" + std::to_string(in[r]) + ";\n";
-                        }
+                        if (cond.empty()) g.s += "    const V " + vname(outid[r]) + " = " + e + ";\n";
+                        else g.s += "    const V " + vname(outid[r]) + " = c" + std::to_string(o) + " ? " + e + " : " +
+                                    vname(in[r]) + ";\n";
                     }
                     for (int r = 0; r < D; ++r) var[s | pdep_c(r, mask)] = outid[r];
                 }
@@ -1654,7 +1716,6 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                     b0 = 1 << nth_bit(op.mask, 0);
                     b1 = 1 << nth_bit(op.mask, 1);
                 }
-                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
                 for (int s = 0; s < E; ++s) {
                     if ((s & op.mask) || !ctrl_ok(s)) continue;
                     const int x0 = var[s | b0], x1 = var[s | b1];
@@ -1671,78 +1732,183 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out) {
                 }
             } else if (op.code == QS_OP_DIAG) {
                 g.add("    // op %d: diagonal, %d register bits, %d other bits\n", o, op.ns, op.nh);
-                if (!cond.empty()) g.add("    const bool c%d = %s;\n", o, cond.c_str());
-                if (op.nh > 0) {
-                    std::string h;
-                    for (int q = 0; q < op.nh; ++q) {
-                        char t[128];
-                        const int src = op.hsrc[q];
-                        if (src < 64) snprintf(t, sizeof(t), "((TH%d >> %d) & 1u)", si, src);
-                        else snprintf(t, sizeof(t), "u32((base >> p.hsh[%d]) & 1ull)", 4 * o + q);
-                        h = h.empty() ? std::string(t) : "((" + h + ") << 1) | " + t;
-                    }
-                    g.add("    const u32 h%d = %s;\n", o, h.c_str());
-                }
+                if (op.nh > 0) g.s += "    const u32 h" + std::to_string(o) + " = " + h_expr(op, o, si) + ";\n";
                 for (int s = 0; s < E; ++s) {
                     if (!ctrl_ok(s)) continue;
                     const int k = op.kidx[s];
                     std::string e;
-                    char t[160];
                     if (op.nh == 0) {
                         const int idx = op.moff + k;
-                        const int cl = vclass(idx);
+                        const int cl = vclass(o, idx);
                         if (cl == 1) continue;
-                        if (cl == 2) snprintf(t, sizeof(t), "cneg(v%d)", var[s]);
-                        else if (cl == 0) snprintf(t, sizeof(t), "%s(0, 0)", MK);
-                        else if (cl == 4) snprintf(t, sizeof(t), "rmul(p.m[%d].x, v%d)", idx, var[s]);
-                        else if (cl == 5) snprintf(t, sizeof(t), "imul(p.m[%d].y, v%d)", idx, var[s]);
-                        else snprintf(t, sizeof(t), "cmul(v%d, p.m[%d])", var[s], idx);
+                        if (cl == 2) e = "cneg(" + vname(var[s]) + ")";
+                        else if (cl == 0) e = std::string(MK) + "(0, 0)";
+                        else if (cl == 4) e = "rmul(" + mref(o, idx) + ".x, " + vname(var[s]) + ")";
+                        else if (cl == 5) e = "imul(" + mref(o, idx) + ".y, " + vname(var[s]) + ")";
+                        else e = "cmul(" + vname(var[s]) + ", " + mref(o, idx) + ")";
                     } else {
-                        snprintf(t, sizeof(t), "cmul(v%d, p.m[%d + ((h%d << %d) | %du)])", var[s], int(op.moff), o,
-                                 int(op.ns), k);
+                        e = "cmul(" + vname(var[s]) + ", " + std::string(strided[o] ? "msm[" : "p.m[") +
+                            std::to_string(int(op.moff)) + " + ((h" + std::to_string(o) + " << " +
+                            std::to_string(int(op.ns)) + ") | " + std::to_string(k) + "u)])";
                     }
-                    e = t;
                     const int nid = fresh++;
-                    if (cond.empty()) g.add("    const V v%d = %s;\n", nid, e.c_str());
-                    else g.add("    const V v%d = c%d ? %s : v%d;\n", nid, o, e.c_str(), var[s]);
+                    if (cond.empty()) g.s += "    const V " + vname(nid) + " = " + e + ";\n";
+                    else g.s += "    const V " + vname(nid) + " = c" + std::to_string(o) + " ? " + e + " : " +
+                                vname(var[s]) + ";\n";
                     var[s] = nid;
                 }
+            } else if (op.code == QS_OP_EXPECT) {
+                // sum over the thread's psi/lam pairs (slot bit 0 = pair bit) of
+                // conj(lam) (G psi) in the state's precision, then a warp sum in FP64
+                if (!cond.empty() || scm != 0 || pair_tile < 0 || S.R[0] != pair_tile) return false;
+                g.add("    { // op %d: <lam| G |psi>\n      S pr = 0, pi = 0;\n", o);
+                const bool dg = op.flags & QS_OPF_DIAG;
+                if (dg && op.nh > 0) g.s += "      const u32 h" + std::to_string(o) + " = " + h_expr(op, o, si) + ";\n";
+                if (dg) {
+                    for (int s = 0; s < E; s += 2) {
+                        const int k = op.kidx[s];
+                        std::string d = op.nh == 0 ? mref(o, op.moff + k)
+                                                   : std::string(strided[o] ? "msm[" : "p.m[") +
+                                                         std::to_string(int(op.moff)) + " + ((h" + std::to_string(o) +
+                                                         " << " + std::to_string(int(op.ns)) + ") | " +
+                                                         std::to_string(k) + "u)]";
+                        g.s += "      { const V acc = cmul(" + d + ", " + vname(var[s]) + "); const V l = " +
+                               vname(var[s | 1]) + ";\n";
+                        g.s += "        pr += l.x * acc.x + l.y * acc.y; pi += l.x * acc.y - l.y * acc.x; }\n";
+                    }
+                } else {
+                    const int mask = op.mask, M = popc_c(mask), D = 1 << M;
+                    if ((mask & 1) || M > 2) return false;
+                    for (int s = 0; s < E; ++s) {
+                        if ((s & mask) || (s & 1)) continue;
+                        int in[4];
+                        for (int c = 0; c < D; ++c) in[c] = var[s | pdep_c(c, mask)];
+                        for (int r = 0; r < D; ++r) {
+                            g.s += "      { const V acc = " + row_expr(o, op.moff + r * D, D, in) + "; const V l = " +
+                                   vname(var[s | 1 | pdep_c(r, mask)]) + ";\n";
+                            g.s += "        pr += l.x * acc.x + l.y * acc.y; pi += l.x * acc.y - l.y * acc.x; }\n";
+                        }
+                    }
+                }
+                g.add("      double re = pr, im = pi;\n");
+                g.add("#pragma unroll\n      for (int off = 16; off > 0; off >>= 1) { re += __shfl_xor_sync(0xffffffffu, "
+                      "re, off); im += __shfl_xor_sync(0xffffffffu, im, off); }\n");
+                g.add("      if ((tid & 31u) == 0) ered[(tid >> 5) * %d + %d] = make_double2(re, im);\n    }\n", NEXP,
+                      int(op.elocal));
             } else {
-                return false;  // EXPECT ops are not generated
+                return false;
             }
         }
     }
     for (int s = 0; s < E; ++s) g.add("    vec[base | gthr | p.gslot[%d]] = v%d;\n", s, var[s]);
+    if (a.nexp > 0) {
+        // per-tile partials: the warps' sums in a fixed order
+        g.add("    __syncthreads();\n");
+        g.add("    for (u32 e = tid; e < %du; e += %du) { double2 t = make_double2(0.0, 0.0);\n", unsigned(a.nexp),
+              threads);
+        g.add("      for (int w = 0; w < %d; ++w) { t.x += ered[w * %d + e].x; t.y += ered[w * %d + e].y; }\n", nwarps,
+              NEXP, NEXP);
+        g.add("      const u64 at = 2 * (p.eslot[e] * ntiles + tile);\n      partials[at] = t.x;\n"
+              "      partials[at + 1] = t.y; }\n");
+    }
     g.add("  }\n}\n");
     if (g.truncated) return false;
     out.src.swap(g.s);
-    out.threads = threads;
-    out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * (size_t(1) << H);
     return true;
+}
+
+// Launch memo: a planned register pass (the used parts of its RegArgs) and its
+// parameter block determine the generated source completely, so repeated
+// launches of the same plan (a replayed circuit, a gradient loop) reuse the
+// loaded kernel without generating and hashing the source again.
+struct JitMemo {
+    std::string src;       // kept until the kernel is ready on some device
+    void* fn[64] = {nullptr};
+    int occ[64] = {0};
+};
+
+uint64_t fnv(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+    return h;
+}
+
+uint64_t plan_key(const RegArgs& a, int R, size_t vsize, const std::vector<uint64_t>& params) {
+    uint64_t h = 1469598103934665603ull;
+    const int hdr[] = {a.n, a.K, a.L, a.H, a.nT, a.nstages, a.nops, a.nmats, a.inst_shift, a.batched, a.nexp,
+                       R, int(vsize)};
+    h = fnv(h, hdr, sizeof(hdr));
+    h = fnv(h, &a.pairmask, sizeof(a.pairmask));
+    h = fnv(h, a.hi, sizeof(int) * size_t(a.H));
+    h = fnv(h, a.eslot, sizeof(int) * size_t(a.nexp));
+    h = fnv(h, a.st, sizeof(KStage) * size_t(a.nstages));
+    h = fnv(h, a.ops, sizeof(KOp) * size_t(a.nops));
+    h = fnv(h, a.cp, sizeof(KCopy) * size_t(a.nops));
+    return fnv(h, params.data(), 8 * params.size());
 }
 
 // Launch the run-time compiled kernel of a planned register pass, if the
 // compiler has it ready (mode SYNC: after compiling it); returns 1 when it
 // was launched, 0 when the generic kernel has to run, < 0 on error.
 template <typename V>
-int launch_jit(V* vec, const RegArgs& args, int R, const V* hm, cudaStream_t st) {
+int launch_jit(V* vec, const RegArgs& args, int R, const V* hm, const V* mats, double* partials, cudaStream_t st) {
     const int jm = jit::mode();
-    if (jm == QS_JIT_OFF || hm == nullptr || args.batched || args.nexp > 0) return 0;
+    if (jm == QS_JIT_OFF || hm == nullptr) return 0;
     static thread_local JitPass jp;
-    if (!gen_reg_pass<V>(args, R, hm, jp)) return 0;
-    void* fn = jit::lookup(jp.src, "qs_pass", jm == QS_JIT_SYNC);
+    if (!gen_reg_pass<V>(args, R, hm, jp, false)) return 0;
+    // during stream capture nothing is compiled or loaded: a kernel that is
+    // not loaded yet on this device leaves the pass to the generic kernel
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    static std::mutex memo_mu;
+    static std::unordered_map<uint64_t, std::shared_ptr<JitMemo>> memo;
+    const uint64_t key = plan_key(args, R, sizeof(V), jp.params);
+    std::shared_ptr<JitMemo> m;
+    {
+        std::lock_guard<std::mutex> lock(memo_mu);
+        auto it = memo.find(key);
+        if (it != memo.end()) m = it->second;
+    }
+    void* fn = m ? m->fn[dev] : nullptr;
+    int occ = m ? m->occ[dev] : 0;
+    if (fn == nullptr) {
+        if (!m) {
+            m = std::make_shared<JitMemo>();
+            JitPass full;
+            if (!gen_reg_pass<V>(args, R, hm, full, true)) return 0;
+            m->src.swap(full.src);
+            std::lock_guard<std::mutex> lock(memo_mu);
+            if (memo.size() > 4096) memo.clear();  // bounded: plans are cheap to regenerate
+            memo[key] = m;
+        }
+        if (m->src.empty()) {  // loaded on another device only: regenerate the text
+            JitPass full;
+            if (!gen_reg_pass<V>(args, R, hm, full, true)) return 0;
+            m->src.swap(full.src);
+        }
+        fn = jit::lookup(m->src, "qs_pass", jm == QS_JIT_SYNC && !capturing, !capturing, jp.threads, jp.smem, &occ);
+        if (fn != nullptr) {
+            std::lock_guard<std::mutex> lock(memo_mu);
+            m->fn[dev] = fn;
+            m->occ[dev] = occ;
+            std::string().swap(m->src);
+        }
+    }
     if (fn == nullptr) {
         jit::count_launch(false);
         return 0;
     }
-    int occ = 0;
-    int rc = jit::occupancy(fn, jp.threads, jp.smem, &occ);
-    if (rc) return rc;
     if (occ < 1) occ = 1;
+    int rc;
     const uint64_t ntiles = uint64_t(1) << (args.n - args.K);
     const uint64_t cap = uint64_t(sm_count()) * uint64_t(occ);
     void* vp = vec;
-    void* params[] = {&vp, jp.params.data()};
+    const void* mp = mats;
+    void* pp = partials;
+    void* params[] = {&vp, jp.params.data(), &mp, &pp};
     rc = jit::launch(fn, unsigned(ntiles < cap ? ntiles : cap), unsigned(jp.threads), jp.smem, st, params);
     if (rc) return rc;
     jit::count_launch(true);
@@ -1776,7 +1942,7 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
             // the generic kernel re-plans the same ops when it is not ready
             std::vector<int> saved = rem;
             if (build_reg(ps, ops, rem, n, RJ, nb, args) > 0) {
-                int jr = launch_jit<V>(vec, args, RJ, hm, st);
+                int jr = launch_jit<V>(vec, args, RJ, hm, mats, partials, st);
                 if (jr < 0) return jr;
                 if (jr == 1) continue;
             }
@@ -1787,8 +1953,8 @@ int launch_reg_k(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* ma
             set_error("qs_apply_fused: op %d does not fit a register tile", next);
             return QS_EINVAL;
         }
-        if (!EXP && RJ == R) {
-            int jr = launch_jit<V>(vec, args, R, hm, st);
+        if (EXP || RJ == R) {
+            int jr = launch_jit<V>(vec, args, R, hm, mats, partials, st);
             if (jr < 0) return jr;
             if (jr == 1) continue;
         }
@@ -1839,8 +2005,8 @@ int launch_reg(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mats
                 return QS_EINVAL;
             }
         }
-        return big ? launch_reg_k<V, R, true, true>(vec, n, ps, ops, mats, partials, st)
-                   : launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st);
+        return big ? launch_reg_k<V, R, true, true>(vec, n, ps, ops, mats, partials, st, hm)
+                   : launch_reg_k<V, R, true, false>(vec, n, ps, ops, mats, partials, st, hm);
     } else {
         return big ? launch_reg_k<V, R, false, true>(vec, n, ps, ops, mats, partials, st, hm)
                    : launch_reg_k<V, R, false, false>(vec, n, ps, ops, mats, partials, st, hm);
@@ -1933,6 +2099,13 @@ extern "C" int qs_adjoint_fused(void* psi, void* lam, int n, int dtype, const qs
 extern "C" int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* passes, int npasses, const qs_op* ops,
                                int64_t nops_total, const void* mats_dev, int64_t mats_count, double* partials_dev,
                                int64_t partials_count, void* stream) {
+    return qs_adjoint_pair_ex(psilam, n, dtype, passes, npasses, ops, nops_total, mats_dev, nullptr, mats_count,
+                              partials_dev, partials_count, stream);
+}
+
+extern "C" int qs_adjoint_pair_ex(void* psilam, int n, int dtype, const qs_pass* passes, int npasses,
+                                  const qs_op* ops, int64_t nops_total, const void* mats_dev, const void* mats_host,
+                                  int64_t mats_count, double* partials_dev, int64_t partials_count, void* stream) {
     QS_REQUIRE(psilam != nullptr, "null vector");
     QS_REQUIRE(n >= 2 && n <= 41, "bit count %d outside [2, 41]", n);
     QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
@@ -1954,10 +2127,10 @@ extern "C" int qs_adjoint_pair(void* psilam, int n, int dtype, const qs_pass* pa
         int rc = dtype == QS_C128
                      ? launch_reg<double2, reg_bits<double2>(), true>((double2*)psilam, n, passes[i], ops,
                                                                       (const double2*)mats_dev, partials_dev,
-                                                                      as_stream(stream))
+                                                                      as_stream(stream), (const double2*)mats_host)
                      : launch_reg<float2, reg_bits<float2>(), true>((float2*)psilam, n, passes[i], ops,
                                                                     (const float2*)mats_dev, partials_dev,
-                                                                    as_stream(stream));
+                                                                    as_stream(stream), (const float2*)mats_host);
         if (rc) return rc;
     }
     return QS_OK;
@@ -1970,7 +2143,8 @@ extern "C" int qs_jit_pass_source(int n, int dtype, const qs_pass* pass, const q
     QS_REQUIRE(valid_dtype(dtype), "bad dtype %d", dtype);
     QS_REQUIRE(pass != nullptr && mats_host != nullptr && src_len != nullptr, "null argument");
     QS_REQUIRE(launch_index >= 0, "negative launch index");
-    int rc = validate_pass(*pass, n, ops, nops_total, mats_count);
+    // pair passes (adjoint) carry EXPECT ops; their partials buffer is not touched here
+    int rc = validate_pass(*pass, n, ops, nops_total, mats_count, pass->pair > 0, INT64_MAX / 4);
     if (rc) return rc;
     const int R = jit_reg_bits(dtype == QS_C128 ? reg_bits<double2>() : reg_bits<float2>());
     const int nT = pass->k - R;

@@ -65,12 +65,15 @@ struct Entry {
     double ms = 0.0;
     void* mod[64] = {nullptr};
     void* fn[64] = {nullptr};
+    int occ[64] = {0};
 };
 
 struct State {
     std::mutex mu;  // guards everything below and the API tables
     std::condition_variable cv;
     Api api;
+    // keyed by a 128-bit hash of the source text (the text itself is kept
+    // only until the entry is compiled)
     std::unordered_map<std::string, std::shared_ptr<Entry>> cache;
     std::deque<std::shared_ptr<Entry>> queue;
     int workers = 0;
@@ -82,6 +85,17 @@ struct State {
     std::atomic<int64_t> compiled{0}, failed{0}, jit_launches{0}, fallback_launches{0}, hits{0};
     std::atomic<int64_t> compile_us{0};
 };
+
+// 128-bit key of a source text: two independent 64-bit FNV-1a hashes.
+std::string source_key(const std::string& src) {
+    uint64_t a = 1469598103934665603ull, b = 0x9e3779b97f4a7c15ull;
+    for (unsigned char c : src) {
+        a = (a ^ c) * 1099511628211ull;
+        b = (b ^ c) * 0x100000001b3ull + 0x632be59bd9b4e019ull;
+    }
+    return std::string(reinterpret_cast<const char*>(&a), 8) + std::string(reinterpret_cast<const char*>(&b), 8) +
+           std::to_string(src.size());
+}
 
 // Never destroyed: worker threads may still run while the process exits.
 State& S() {
@@ -169,6 +183,7 @@ void compile_entry(State& s, Entry& e) {
         e.cubin.swap(cubin);
         e.state = 1;
         ++s.compiled;
+        std::string().swap(e.src);  // the cache keeps the hash, not the text
     } else {
         e.state = 2;
         ++s.failed;
@@ -183,9 +198,11 @@ void worker_loop() {
     for (;;) {
         std::shared_ptr<Entry> e;
         {
+            // after shutdown_workers the thread parks here until the process
+            // ends: a returning thread would run the compiler library's
+            // thread-exit hooks while the process is unloading that library
             std::unique_lock<std::mutex> lock(s.mu);
-            s.cv.wait(lock, [&] { return !s.queue.empty() || s.stopping; });
-            if (s.stopping) return;
+            s.cv.wait(lock, [&] { return !s.queue.empty() && !s.stopping; });
             e = s.queue.front();
             s.queue.pop_front();
             ++s.running;
@@ -198,10 +215,12 @@ void worker_loop() {
 }
 
 // At process exit: drop queued work and let running compilations finish, so
-// no worker is inside NVRTC while the process tears its libraries down.
+// no worker is inside NVRTC while the process tears its libraries down (the
+// idle workers stay parked; the process ends them).
 void shutdown_workers() {
     State& s = S();
     std::unique_lock<std::mutex> lock(s.mu);
+    if (s.stopping && s.running == 0) return;
     s.stopping = true;
     for (auto& e : s.queue) e->state = 2;
     s.pending -= int(s.queue.size());
@@ -220,12 +239,16 @@ void start_workers(State& s) {  // with s.mu held
     std::atexit(shutdown_workers);
 }
 
-// Loaded function of a ready entry on the current device (with s.mu held).
-void* device_function(State& s, Entry& e) {
+// Loaded function of a ready entry on the current device (with s.mu held);
+// loads it when `load` allows.
+void* device_function(State& s, Entry& e, bool load, int threads, size_t smem, int* occ) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    if (e.fn[dev]) return e.fn[dev];
-    if (!load_driver(s)) return nullptr;
+    if (e.fn[dev]) {
+        *occ = e.occ[dev];
+        return e.fn[dev];
+    }
+    if (!load || !load_driver(s)) return nullptr;
     cudaFree(nullptr);  // the runtime's primary context is current from here on
     CUmodule mod = nullptr;
     CUresult r = s.api.module_load(&mod, e.cubin.data());
@@ -246,8 +269,16 @@ void* device_function(State& s, Entry& e) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (optin > 0) s.api.set_attr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, optin);
+    int nb = 0;
+    if (s.api.occupancy(&nb, fn, threads, smem) != CUDA_SUCCESS || nb < 1) {
+        s.last_log = "cuOccupancyMaxActiveBlocksPerMultiprocessor: the kernel does not fit an SM";
+        e.state = 2;
+        return nullptr;
+    }
     e.mod[dev] = mod;
     e.fn[dev] = fn;
+    e.occ[dev] = nb;
+    *occ = nb;
     return fn;
 }
 
@@ -267,19 +298,30 @@ int mode() {
 
 void set_mode(int m) { S().mode = m; }
 
-void* lookup(const std::string& src, const char* name, bool block) {
+void shutdown() {
+    State& s = S();
+    {
+        std::lock_guard<std::mutex> lock(s.mu);
+        if (s.workers == 0) return;
+    }
+    shutdown_workers();
+}
+
+void* lookup(const std::string& src, const char* name, bool block, bool load, int threads, size_t smem, int* occ) {
     State& s = S();
     std::shared_ptr<Entry> e;
     bool compile_here = false;
     {
         std::unique_lock<std::mutex> lock(s.mu);
         if (!load_nvrtc(s)) return nullptr;
-        auto it = s.cache.find(src);
+        const std::string key = source_key(src);
+        if (s.stopping && s.cache.find(key) == s.cache.end()) return nullptr;  // shut down: nothing new
+        auto it = s.cache.find(key);
         if (it == s.cache.end()) {
             e = std::make_shared<Entry>();
             e->src = src;
             e->name = name;
-            s.cache.emplace(src, e);
+            s.cache.emplace(key, e);
             ++s.pending;
             if (block) {
                 compile_here = true;
@@ -296,13 +338,13 @@ void* lookup(const std::string& src, const char* name, bool block) {
             if (e->state == 0 && block) s.cv.wait(lock, [&] { return e->state != 0; });
             if (e->state != 1) return nullptr;
             ++s.hits;
-            return device_function(s, *e);
+            return device_function(s, *e, load, threads, smem, occ);
         }
     }
     compile_entry(s, *e);
     std::lock_guard<std::mutex> lock(s.mu);
     if (e->state != 1) return nullptr;
-    return device_function(s, *e);
+    return device_function(s, *e, load, threads, smem, occ);
 }
 
 int launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st, void** params) {
@@ -313,16 +355,6 @@ int launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st
         const char* m = nullptr;
         s.api.cu_err(r, &m);
         set_error("cuLaunchKernel (compiled pass): %s", m ? m : "error");
-        return QS_ECUDA;
-    }
-    return QS_OK;
-}
-
-int occupancy(void* fn, int block, size_t smem, int* out) {
-    State& s = S();
-    CUresult r = s.api.occupancy(out, static_cast<CUfunction>(fn), block, smem);
-    if (r != CUDA_SUCCESS) {
-        set_error("cuOccupancyMaxActiveBlocksPerMultiprocessor failed (%d)", int(r));
         return QS_ECUDA;
     }
     return QS_OK;
@@ -406,6 +438,11 @@ int compile_check(const char* src, int64_t* cubin_bytes, std::string* log) {
 
 }  // namespace jit
 }  // namespace qs
+
+extern "C" int qs_jit_shutdown(void) {
+    qs::jit::shutdown();
+    return QS_OK;
+}
 
 extern "C" int qs_jit_set_mode(int mode) {
     if (mode < QS_JIT_OFF || mode > QS_JIT_SYNC) {

@@ -22,15 +22,15 @@ void set_mode(int m);
 // (mode ASYNC: the call returns null until it is done) or compiled before
 // returning (mode SYNC, or `block`).  Null when compilation failed; the
 // first failure's log is kept for qs_jit_last_log.
-void* lookup(const std::string& src, const char* name, bool block);
+// `load`: allow loading the cubin on this device now (false during stream
+// capture: then only an already loaded kernel is returned).  *occ <- resident
+// blocks per SM at `threads` threads and `smem` dynamic shared memory
+// (computed when the kernel is loaded).
+void* lookup(const std::string& src, const char* name, bool block, bool load, int threads, size_t smem, int* occ);
 
 // cuLaunchKernel of a looked-up function; `params` points to the kernel's
 // parameter values (one pointer per kernel argument).
 int launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st, void** params);
-
-// Resident blocks per SM for `fn` at `block` threads and `smem` dynamic
-// shared memory (after opting it into that much shared memory).
-int occupancy(void* fn, int block, size_t smem, int* out);
 
 // Wait for every queued compilation (seconds; < 0: no limit).  QS_ETIMEOUT
 // when the limit passed first.
@@ -41,6 +41,9 @@ int wait_all(double timeout_s);
 // the generic kernel while a compilation was pending, [5] total compile
 // milliseconds, [6] cache hits on a compiled kernel.
 void stats(int64_t* out, int n);
+// Drop queued compilations and wait for running ones; later lookups of new
+// sources stay uncompiled (the generic kernels run them).
+void shutdown();
 void count_launch(bool compiled);
 const char* last_log();
 

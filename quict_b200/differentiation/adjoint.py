@@ -166,7 +166,7 @@ class BatchedAdjoint:
 
     def __init__(self, circuit: ParamCircuit, observable: PauliSum, precision: str = "single",
                  device_id: int = 0, tile_bits: Optional[int] = None, pair: bool = True,
-                 pair_tile_bits: Optional[int] = None):
+                 pair_tile_bits: Optional[int] = None, jit: bool = True):
         if observable.n != circuit.n:
             raise ValueError("observable and circuit act on different qubit counts")
         k0, _ = default_tile(8 if precision == "single" else 16)
@@ -190,6 +190,9 @@ class BatchedAdjoint:
         self.pair_k = pair_tile_bits or min(k0, max(min_k, self.n + 1 - 3))
         self.pair_min_k = min_k
         self.pair = pair and self.pair_min_k <= self.pair_k <= self.n + 1
+        # jit: register passes may run as run-time compiled kernels (the
+        # library's JIT mode decides when); False keeps the generic kernels
+        self.jit = jit
         self.ws = Workspace(self.dev)
         self.launches = 0
         self.pauli = observable.masks()
@@ -230,10 +233,12 @@ class BatchedAdjoint:
             raise RuntimeError("a gradient-circuit op could not be fused")
         table = MatrixTable()
         cps, npass, cops, nops = emit(passes, table, inst_shift=self.n)
-        mats = torch.from_numpy(table.array().astype(self.np_dtype)).to(self.dev)
+        host = table.array().astype(self.np_dtype)
+        mats = torch.from_numpy(host).to(self.dev)
         if lam is None:
-            N.call("qs_apply_fused", C.c_void_p(vec.data_ptr()), nbits, qs_dtype(vec), cps, npass, cops, nops,
-                   C.c_void_p(mats.data_ptr()), int(mats.numel()), self.stream)
+            hp = C.c_void_p(host.ctypes.data) if self.jit else None
+            N.call("qs_apply_fused_ex", C.c_void_p(vec.data_ptr()), nbits, qs_dtype(vec), cps, npass, cops, nops,
+                   C.c_void_p(mats.data_ptr()), hp, int(mats.numel()), self.stream)
         else:
             N.call("qs_adjoint_fused", C.c_void_p(vec.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
                    qs_dtype(vec), cps, npass, cops, nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
@@ -345,8 +350,10 @@ class BatchedAdjoint:
             raise RuntimeError("a gradient-circuit op could not be fused")
         table = MatrixTable()
         cps, npass, cops, nops = emit(passes, table, inst_shift=self.n, pair=pair)
-        mats = torch.from_numpy(table.array().astype(self.np_dtype)).to(self.dev)
-        return (cps, npass, cops, nops, mats)
+        host = table.array().astype(self.np_dtype)
+        mats = torch.from_numpy(host).to(self.dev)
+        # the host copy lets register passes run as generated kernels
+        return (cps, npass, cops, nops, mats, host)
 
     def launch(self, gp: "GradientPlan", stream=None):
         """Issue the forward, energy and adjoint kernels of a plan on `stream`
@@ -356,19 +363,21 @@ class BatchedAdjoint:
         psi, lam = gp.psi, gp.lam
         psi.zero_()
         psi.view(bp, 1 << n)[:, 0] = 1
-        cps, npass, cops, nops, mats = gp.fwd
-        N.call("qs_apply_fused", C.c_void_p(psi.data_ptr()), nbits, qs_dtype(psi), cps, npass, cops, nops,
-               C.c_void_p(mats.data_ptr()), int(mats.numel()), st)
+        cps, npass, cops, nops, mats, host = gp.fwd
+        hp = C.c_void_p(host.ctypes.data) if self.jit else None
+        N.call("qs_apply_fused_ex", C.c_void_p(psi.data_ptr()), nbits, qs_dtype(psi), cps, npass, cops, nops,
+               C.c_void_p(mats.data_ptr()), hp, int(mats.numel()), st)
         x, z, c = self.pauli
         N.call("qs_apply_pauli_sum", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,
                qs_dtype(psi), x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
                c.ctypes.data_as(C.c_void_p), len(x), st)
         N.call("qs_inner_batched", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits, qs_dtype(psi),
                n, C.c_void_p(gp.e.data_ptr()), C.c_void_p(gp.ws.data_ptr()), gp.ws.numel(), st)
-        cps, npass2, cops, nops, mats = gp.bwd
+        cps, npass2, cops, nops, mats, host = gp.bwd
         if gp.pair:
-            N.call("qs_adjoint_pair", C.c_void_p(gp.pl.data_ptr()), nbits + 1, qs_dtype(psi), cps, npass2, cops,
-                   nops, C.c_void_p(mats.data_ptr()), int(mats.numel()),
+            hp = C.c_void_p(host.ctypes.data) if self.jit else None
+            N.call("qs_adjoint_pair_ex", C.c_void_p(gp.pl.data_ptr()), nbits + 1, qs_dtype(psi), cps, npass2, cops,
+                   nops, C.c_void_p(mats.data_ptr()), hp, int(mats.numel()),
                    C.c_void_p(gp.partials.data_ptr()), int(gp.partials.numel()), st)
         else:
             N.call("qs_adjoint_fused", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits,

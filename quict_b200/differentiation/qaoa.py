@@ -37,9 +37,16 @@ def qaoa_instances(count: int = 512, sizes: Sequence[int] = tuple(range(10, 25, 
 
 
 class UnevenQAOABatch:
-    def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16):
+    """`jit_min_qubits`: instances of at least that many qubits run their
+    register passes as run-time compiled kernels (their kernels dominate the
+    replay); smaller ones keep the generic kernels, whose per-instance
+    compilation would not pay off."""
+
+    def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16,
+                 jit_min_qubits: int = 22):
         self.instances = instances
-        self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id)
+        self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id,
+                                       jit=n >= jit_min_qubits)
                         for n, edges, p, _ in instances]
         self.plans: List[GradientPlan] = [eng.plan_gradient(np.asarray(prm)[None, :])
                                           for eng, (_, _, _, prm) in zip(self.engines, instances)]
@@ -69,9 +76,13 @@ class UnevenQAOABatch:
         self._launch_all(streams)
 
     def capture(self):
-        """Warm up once (first-launch configuration happens outside capture),
-        then capture every instance's chain into one CUDA graph."""
+        """Warm up (first-launch configuration and the compilation of the
+        generated pass kernels happen outside capture), then capture every
+        instance's chain into one CUDA graph."""
+        from .. import _native as N
         self.run_eager()
+        N.jit_wait(900)
+        self.run_eager()  # loads the compiled kernels on this device
         torch.cuda.synchronize(self.dev)
         self.graph = torch.cuda.CUDAGraph()
         streams = [torch.cuda.Stream(self.dev) for _ in range(self.nstreams)]

@@ -174,3 +174,38 @@ def test_async_mode_switches_to_compiled_kernels(cuda_ok):
         np.testing.assert_allclose(v2, ref, rtol=0, atol=1e-12)
     finally:
         N.jit_set_mode(prev)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("double", 1e-10), ("single", 1e-4)])
+def test_compiled_adjoint_passes_match_generic_kernels(cuda_ok, precision, tol):
+    """Batched forward passes (per-instance tables staged in shared memory) and
+    adjoint pair passes (EXPECT partials) as generated kernels, against the
+    generic kernels: a hardware-efficient-ansatz batch and a QAOA instance."""
+    from quict_b200 import _native as N
+    from quict_b200.differentiation import (BatchedAdjoint, hardware_efficient_ansatz, ising_observable,
+                                            maxcut_observable, qaoa_circuit, random_regular_graph)
+    circ, obs = hardware_efficient_ansatz(13, 2), ising_observable(13)
+    params = np.random.default_rng(8).uniform(0, 2 * np.pi, (4, circ.num_params))
+    edges = random_regular_graph(16, 3, np.random.default_rng(3))
+    qc, qo = qaoa_circuit(16, edges, 3), maxcut_observable(16, edges)
+    prm = np.random.default_rng(9).uniform(0, 3, (1, qc.num_params))
+    prev = N.jit_set_mode(N.QS_JIT_OFF)
+    try:
+        want = [BatchedAdjoint(circ, obs, precision).gradient(params),
+                BatchedAdjoint(qc, qo, precision).gradient(prm)]
+        N.jit_set_mode(N.QS_JIT_ASYNC)  # compile every shape on the pool, then run them compiled
+        for c, o, p in ((circ, obs, params), (qc, qo, prm)):
+            BatchedAdjoint(c, o, precision).gradient(p)
+        N.jit_wait(900)
+        N.jit_set_mode(N.QS_JIT_SYNC)
+        before = N.jit_stats()
+        got = [BatchedAdjoint(circ, obs, precision).gradient(params),
+               BatchedAdjoint(qc, qo, precision).gradient(prm)]
+        after = N.jit_stats()
+    finally:
+        N.jit_set_mode(prev)
+    assert after["compiled_launches"] > before["compiled_launches"] and after["failed"] == before["failed"]
+    for (e0, g0), (e1, g1), scale in zip(want, got, (1.0, float(len(edges)))):
+        np.testing.assert_allclose(e1.cpu().numpy(), e0.cpu().numpy(), rtol=0, atol=tol * scale)
+        np.testing.assert_allclose(g1.cpu().numpy(), g0.cpu().numpy(), rtol=0, atol=4 * tol * scale)
