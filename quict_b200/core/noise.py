@@ -253,6 +253,7 @@ class NoiseModel:
         self._basic_gates = list(basic_gates) if basic_gates is not None else list(self._BASED_GATES)
         self._error_by_gate = {g: [] for g in self._basic_gates}
         self._readout_errors: List[Tuple[ReadoutError, List[int]]] = []
+        self._version = 0  # bumped by every change (simulators key cached lowerings on it)
 
     def add(self, noise: QuantumNoiseError, gates: Union[str, List[str]], qubits=None):
         gates = [gates] if isinstance(gates, str) else list(gates)
@@ -261,6 +262,7 @@ class NoiseModel:
                 raise ValueError(f"gate {g} is not in the noise model's basic gates")
             self._error_by_gate[g].append((noise, -1 if qubits is None else
                                            ([qubits] if isinstance(qubits, int) else list(qubits))))
+        self._version += 1
 
     def add_noise_for_all_qubits(self, noise: QuantumNoiseError, gates: Union[str, List[str]]):
         self.add(noise, gates, None)
@@ -270,6 +272,7 @@ class NoiseModel:
         if noise.qubits > 1 and noise.qubits != len(qubits):
             raise ValueError("multi-qubit readout error needs exactly its qubit count")
         self._readout_errors.append((noise, qubits))
+        self._version += 1
 
     def transpile(self, circuit, accumulated_mode: bool = False, rng=np.random):
         from .circuit import Circuit

@@ -1390,6 +1390,7 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
 struct JitPass {
     std::string src;
     std::vector<uint64_t> params;  // the kernel's parameter block (16-byte multiple)
+    std::vector<uint8_t> classes;  // value class of every matrix entry (what the source depends on)
     int threads = 0;
     size_t smem = 0;
 };
@@ -1519,6 +1520,12 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     auto mref = [&](int o, int idx) -> std::string {
         return (strided[o] ? "msm[" : "p.m[") + std::to_string(idx) + "]";
     };
+    out.classes.resize(size_t(NM));
+    for (int o = 0; o < a.nops; ++o) {
+        const KCopy& c = a.cp[o];
+        const int cnt = c.diag ? (1 << c.m) : (1 << (2 * c.m));
+        for (int e = 0; e < cnt; ++e) out.classes[c.soff + e] = uint8_t(vclass(o, c.soff + e));
+    }
     const unsigned hoff_n = (1u << H) < 2u ? 2u : (1u << H);  // a 16-byte multiple
     out.threads = threads;
     out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * size_t(hoff_n) +
@@ -1833,7 +1840,10 @@ uint64_t fnv(uint64_t h, const void* p, size_t n) {
     return h;
 }
 
-uint64_t plan_key(const RegArgs& a, int R, size_t vsize, const std::vector<uint64_t>& params) {
+// The source depends on the plan's structure and on the entries' value
+// classes, not on the matrix values: the key hashes exactly those, so a new
+// parameter set of the same circuit reuses the compiled kernel.
+uint64_t plan_key(const RegArgs& a, int R, size_t vsize, const std::vector<uint8_t>& classes) {
     uint64_t h = 1469598103934665603ull;
     const int hdr[] = {a.n, a.K, a.L, a.H, a.nT, a.nstages, a.nops, a.nmats, a.inst_shift, a.batched, a.nexp,
                        R, int(vsize)};
@@ -1843,8 +1853,18 @@ uint64_t plan_key(const RegArgs& a, int R, size_t vsize, const std::vector<uint6
     h = fnv(h, a.eslot, sizeof(int) * size_t(a.nexp));
     h = fnv(h, a.st, sizeof(KStage) * size_t(a.nstages));
     h = fnv(h, a.ops, sizeof(KOp) * size_t(a.nops));
-    h = fnv(h, a.cp, sizeof(KCopy) * size_t(a.nops));
-    return fnv(h, params.data(), 8 * params.size());
+    for (int o = 0; o < a.nops; ++o) {  // the table layout, not where the tables sit (goff)
+        const KCopy& c = a.cp[o];
+        const int f[] = {int(c.soff), int(c.m), int(c.diag), int(c.stride != 0), c.perm[0], c.perm[1], c.perm[2],
+                         c.perm[3]};
+        h = fnv(h, f, sizeof(f));
+    }
+    static const int target = [] {
+        const char* e = getenv("QS_JIT_THREADS_PER_SM");
+        return e && *e ? atoi(e) : 0;
+    }();
+    h = fnv(h, &target, sizeof(target));
+    return fnv(h, classes.data(), classes.size());
 }
 
 // Launch the run-time compiled kernel of a planned register pass, if the
@@ -1865,7 +1885,7 @@ int launch_jit(V* vec, const RegArgs& args, int R, const V* hm, const V* mats, d
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
     static std::mutex memo_mu;
     static std::unordered_map<uint64_t, std::shared_ptr<JitMemo>> memo;
-    const uint64_t key = plan_key(args, R, sizeof(V), jp.params);
+    const uint64_t key = plan_key(args, R, sizeof(V), jp.classes);
     std::shared_ptr<JitMemo> m;
     {
         std::lock_guard<std::mutex> lock(memo_mu);

@@ -88,6 +88,87 @@ k_1q_pair(V* __restrict__ v, uint64_t items, Plan plan, uint64_t cmask, uint64_t
     }
 }
 
+// complex64, target and control bits >= 1: two adjacent work items are two
+// adjacent amplitudes, so each thread moves float4s (128-bit accesses).
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_1q_pair_v2(float2* __restrict__ v, uint64_t items2, Plan plan, uint64_t cmask, uint64_t off, Mat<float2, 4> M) {
+    const uint64_t step = uint64_t(gridDim.x) * kThreads * kUnroll;
+    float4* __restrict__ v4 = reinterpret_cast<float4*>(v);
+    const uint64_t off4 = off >> 1;
+    for (uint64_t j0 = uint64_t(blockIdx.x) * kThreads * kUnroll + threadIdx.x; j0 < items2; j0 += step) {
+        float4 a[kUnroll], b[kUnroll];
+        uint64_t q[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j < items2) {
+                q[u] = (expand(2 * j, plan) | cmask) >> 1;  // even amplitude index -> float4 index
+                a[u] = v4[q[u]];
+                b[u] = v4[q[u] + off4];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j >= items2) continue;
+            const float2 a0 = make_float2(a[u].x, a[u].y), a1 = make_float2(a[u].z, a[u].w);
+            const float2 b0 = make_float2(b[u].x, b[u].y), b1 = make_float2(b[u].z, b[u].w);
+            float2 x0, y0, x1, y1;
+            if (KIND == QS_K_DENSE) {
+                x0 = cfma(M.m[0], a0, cmul(M.m[1], b0));
+                y0 = cfma(M.m[2], a0, cmul(M.m[3], b0));
+                x1 = cfma(M.m[0], a1, cmul(M.m[1], b1));
+                y1 = cfma(M.m[2], a1, cmul(M.m[3], b1));
+            } else {
+                x0 = cmul(M.m[1], b0);
+                y0 = cmul(M.m[2], a0);
+                x1 = cmul(M.m[1], b1);
+                y1 = cmul(M.m[2], a1);
+            }
+            v4[q[u]] = make_float4(x0.x, x0.y, x1.x, x1.y);
+            v4[q[u] + off4] = make_float4(y0.x, y0.y, y1.x, y1.y);
+        }
+    }
+}
+
+// complex64 diagonal with 128-bit accesses: bit 0 is neither fixed nor the
+// selector's `hi` bit, so each float4 holds a pair (even, odd) of amplitudes.
+__global__ void __launch_bounds__(kThreads)
+k_diag_v2(float2* __restrict__ v, uint64_t items2, Plan plan, uint64_t fixed, int bhi, int blo, Mat<float2, 4> D) {
+    const uint64_t step = uint64_t(gridDim.x) * kThreads * kUnroll;
+    float4* __restrict__ v4 = reinterpret_cast<float4*>(v);
+    for (uint64_t j0 = uint64_t(blockIdx.x) * kThreads * kUnroll + threadIdx.x; j0 < items2; j0 += step) {
+        float4 a[kUnroll];
+        uint64_t idx[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j < items2) {
+                idx[u] = expand(2 * j, plan) | fixed;
+                a[u] = v4[idx[u] >> 1];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j >= items2) continue;
+            int s0 = 0, s1 = 0;
+            if (bhi >= 0) s0 = s1 = int((idx[u] >> bhi) & 1) << 1;
+            if (blo == 0) {
+                s1 |= 1;
+            } else if (blo > 0) {
+                const int b = int((idx[u] >> blo) & 1);
+                s0 |= b;
+                s1 |= b;
+            }
+            const float2 y0 = cmul(make_float2(a[u].x, a[u].y), D.m[s0]);
+            const float2 y1 = cmul(make_float2(a[u].z, a[u].w), D.m[s1]);
+            v4[idx[u] >> 1] = make_float4(y0.x, y0.y, y1.x, y1.y);
+        }
+    }
+}
+
 // ------------------------------------------------------------ 1q, shuffles
 // Target bit < 5 and n >= 5.  Each warp owns 32 consecutive amplitudes of the
 // compact space (control bits >= 5 removed); lane partner = lane ^ (1<<bit).
@@ -165,33 +246,46 @@ template <typename V, int KIND>
 __global__ void __launch_bounds__(kThreads)
 k_2q_quad(V* __restrict__ v, uint64_t items, Plan plan, uint64_t cmask, uint64_t ohi, uint64_t olo,
           Mat<V, 16> M, bool touch_diag) {
-    const uint64_t step = uint64_t(gridDim.x) * kThreads * 2;
-    for (uint64_t j0 = uint64_t(blockIdx.x) * kThreads * 2 + threadIdx.x; j0 < items; j0 += step) {
+    // four quads per thread, all loads issued before any store: 16 (dense)
+    // or 8 (swap) independent loads in flight per thread
+    constexpr int U = 4;
+    const uint64_t step = uint64_t(gridDim.x) * kThreads * U;
+    for (uint64_t j0 = uint64_t(blockIdx.x) * kThreads * U + threadIdx.x; j0 < items; j0 += step) {
+        uint64_t i00[U];
+        V x[U][4];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            uint64_t j = j0 + uint64_t(u) * kThreads;
-            if (j >= items) break;
-            uint64_t i00 = expand(j, plan) | cmask;
-            uint64_t i01 = i00 | olo, i10 = i00 | ohi, i11 = i00 | ohi | olo;
+        for (int u = 0; u < U; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j < items) {
+                i00[u] = expand(j, plan) | cmask;
+                if (KIND == QS_K_DENSE || touch_diag) x[u][0] = v[i00[u]];
+                x[u][1] = v[i00[u] | olo];
+                x[u][2] = v[i00[u] | ohi];
+                if (KIND == QS_K_DENSE || touch_diag) x[u][3] = v[i00[u] | ohi | olo];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t j = j0 + uint64_t(u) * kThreads;
+            if (j >= items) continue;
+            const uint64_t i01 = i00[u] | olo, i10 = i00[u] | ohi, i11 = i00[u] | ohi | olo;
             if (KIND == QS_K_DENSE) {
-                V x0 = v[i00], x1 = v[i01], x2 = v[i10], x3 = v[i11];
                 V y[4];
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    V acc = cmul(M.m[4 * r + 0], x0);
-                    acc = cfma(M.m[4 * r + 1], x1, acc);
-                    acc = cfma(M.m[4 * r + 2], x2, acc);
-                    acc = cfma(M.m[4 * r + 3], x3, acc);
+                    V acc = cmul(M.m[4 * r + 0], x[u][0]);
+                    acc = cfma(M.m[4 * r + 1], x[u][1], acc);
+                    acc = cfma(M.m[4 * r + 2], x[u][2], acc);
+                    acc = cfma(M.m[4 * r + 3], x[u][3], acc);
                     y[r] = acc;
                 }
-                v[i00] = y[0]; v[i01] = y[1]; v[i10] = y[2]; v[i11] = y[3];
+                v[i00[u]] = y[0]; v[i01] = y[1]; v[i10] = y[2]; v[i11] = y[3];
             } else {  // QS_K_SWAP
-                V x1 = v[i01], x2 = v[i10];
-                v[i01] = cmul(M.m[6], x2);
-                v[i10] = cmul(M.m[9], x1);
+                v[i01] = cmul(M.m[6], x[u][2]);
+                v[i10] = cmul(M.m[9], x[u][1]);
                 if (touch_diag) {
-                    v[i00] = cmul(M.m[0], v[i00]);
-                    v[i11] = cmul(M.m[15], v[i11]);
+                    v[i00[u]] = cmul(M.m[0], x[u][0]);
+                    v[i11] = cmul(M.m[15], x[u][3]);
                 }
             }
         }
@@ -275,6 +369,22 @@ int check_common(void* vec, int n, int dtype) {
     return QS_OK;
 }
 
+// Diagonal launch: complex64 pairs of adjacent amplitudes move as float4
+// when bit 0 is neither fixed nor the selector's high bit.
+template <typename V>
+void launch_diag(V* v, uint64_t items, const Plan& p, uint64_t fixed, int bhi, int blo, const Mat<V, 4>& D,
+                 cudaStream_t st) {
+    if constexpr (sizeof(V) == 8) {
+        if (!(fixed & 1) && bhi != 0 && items >= 2) {
+            const uint64_t items2 = items >> 1;
+            k_diag_v2<<<grid_for(items2, kThreads * kUnroll, 8), kThreads, 0, st>>>((float2*)v, items2, p, fixed, bhi,
+                                                                                   blo, D);
+            return;
+        }
+    }
+    k_diag<V><<<grid_for(items, kThreads * kUnroll, 8), kThreads, 0, st>>>(v, items, p, fixed, bhi, blo, D);
+}
+
 template <typename R>
 int apply_1q_t(void* vec, int n, int bit, uint64_t cmask, int kind, const double* mat, cudaStream_t st) {
     using V = typename CT<R>::V;
@@ -289,7 +399,7 @@ int apply_1q_t(void* vec, int n, int bit, uint64_t cmask, int kind, const double
         uint64_t items = uint64_t(1) << (n - p.nb);
         Mat<V, 4> D;
         D.m[0] = M.m[0]; D.m[1] = M.m[3]; D.m[2] = M.m[0]; D.m[3] = M.m[3];
-        k_diag<V><<<grid_for(items, kThreads * kUnroll, 8), kThreads, 0, st>>>(v, items, p, fixed, -1, bit, D);
+        launch_diag<V>(v, items, p, fixed, -1, bit, D, st);
         QS_CHECK_LAUNCH("qs_apply_1q(diag)");
         return QS_OK;
     }
@@ -307,6 +417,18 @@ int apply_1q_t(void* vec, int n, int bit, uint64_t cmask, int kind, const double
     }
     Plan p = make_plan(cmask | tbit);
     uint64_t items = uint64_t(1) << (n - p.nb);
+    if constexpr (sizeof(V) == 8) {
+        if (!(cmask & 1) && bit >= 1 && items >= 2) {  // adjacent amplitude pairs: float4 accesses
+            const uint64_t items2 = items >> 1;
+            unsigned grid2 = grid_for(items2, kThreads * kUnroll, 8);
+            if (kind == QS_K_DENSE)
+                k_1q_pair_v2<QS_K_DENSE><<<grid2, kThreads, 0, st>>>((float2*)v, items2, p, cmask, tbit, M);
+            else
+                k_1q_pair_v2<QS_K_ANTIDIAG><<<grid2, kThreads, 0, st>>>((float2*)v, items2, p, cmask, tbit, M);
+            QS_CHECK_LAUNCH("qs_apply_1q(pair, float4)");
+            return QS_OK;
+        }
+    }
     unsigned grid = grid_for(items, kThreads * kUnroll, 8);
     if (kind == QS_K_DENSE)
         k_1q_pair<V, QS_K_DENSE><<<grid, kThreads, 0, st>>>(v, items, p, cmask, tbit, M);
@@ -327,13 +449,13 @@ int apply_2q_t(void* vec, int n, int bhi, int blo, uint64_t cmask, int kind, con
         uint64_t items = uint64_t(1) << (n - p.nb);
         Mat<V, 4> D;
         D.m[0] = M.m[0]; D.m[1] = M.m[5]; D.m[2] = M.m[10]; D.m[3] = M.m[15];
-        k_diag<V><<<grid_for(items, kThreads * kUnroll, 8), kThreads, 0, st>>>(v, items, p, cmask, bhi, blo, D);
+        launch_diag<V>(v, items, p, cmask, bhi, blo, D, st);
         QS_CHECK_LAUNCH("qs_apply_2q(diag)");
         return QS_OK;
     }
     Plan p = make_plan(cmask | ohi | olo);
     uint64_t items = uint64_t(1) << (n - p.nb);
-    unsigned grid = grid_for(items, kThreads * 2, 8);
+    unsigned grid = grid_for(items, kThreads * 4, 8);
     if (kind == QS_K_DENSE) {
         k_2q_quad<V, QS_K_DENSE><<<grid, kThreads, 0, st>>>(v, items, p, cmask, ohi, olo, M, true);
     } else {

@@ -45,9 +45,11 @@ class UnevenQAOABatch:
     def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16,
                  jit_min_qubits: int = 22):
         self.instances = instances
+        self.jit_min_qubits = jit_min_qubits
         self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id,
                                        jit=n >= jit_min_qubits)
                         for n, edges, p, _ in instances]
+        self.captured_launches = 0  # kernel launches recorded in the graph
         self.plans: List[GradientPlan] = [eng.plan_gradient(np.asarray(prm)[None, :])
                                           for eng, (_, _, _, prm) in zip(self.engines, instances)]
         self.dev = self.engines[0].dev if self.engines else torch.device("cuda", device_id)
@@ -86,8 +88,10 @@ class UnevenQAOABatch:
         torch.cuda.synchronize(self.dev)
         self.graph = torch.cuda.CUDAGraph()
         streams = [torch.cuda.Stream(self.dev) for _ in range(self.nstreams)]
+        before = sum(e.launches for e in self.engines)
         with torch.cuda.graph(self.graph):
             self._launch_all(streams)
+        self.captured_launches = sum(e.launches for e in self.engines) - before
         return self.graph
 
     def replay(self):

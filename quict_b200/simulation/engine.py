@@ -7,6 +7,7 @@ CUDA device or library raises.
 from __future__ import annotations
 
 import ctypes as C
+from collections import OrderedDict
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -36,6 +37,34 @@ def require_cuda(device_id: int = 0) -> torch.device:
     if not torch.cuda.is_available():
         raise RuntimeError("quict_b200 simulators need a CUDA device; none is visible (no CPU fallback)")
     return torch.device("cuda", device_id)
+
+
+class _Program:
+    """Replayable plan of an op sequence: segments ("passes", qs_pass[],
+    npass, qs_op[], nops, host table, pinned copy of the table) for runs of
+    fused passes and ("single", op) for ops the per-gate kernels apply."""
+
+    def __init__(self, steps, tdtype: torch.dtype):
+        npd = np.complex64 if tdtype == torch.complex64 else np.complex128
+        self.segments = []
+        run: List[Pass] = []
+
+        def flush():
+            if run:
+                table = MatrixTable()
+                cps, npass, cops, nops = emit(run, table)
+                host = table.array().astype(npd)
+                self.segments.append(("passes", cps, npass, cops, nops, host, torch.from_numpy(host).pin_memory()))
+                run.clear()
+
+        for st in steps:
+            if isinstance(st, Pass):
+                if st.ops:
+                    run.append(st)
+            else:
+                flush()
+                self.segments.append(("single", st.op))
+        flush()
 
 
 class Workspace:
@@ -72,6 +101,9 @@ class Engine:
         self.launches = 0  # libqsim kernel launches issued (per gate or per fused pass)
         self.h2d_bytes = 0  # host->device bytes copied for matrix tables
         self.pass_events = None  # list -> record (start, end, nops) CUDA events per fused pass
+        # planned programs of recently applied op sequences (see apply_ops)
+        self.programs: "OrderedDict[tuple, _Program]" = OrderedDict()
+        self.max_programs = 8
 
     @property
     def stream(self):
@@ -172,18 +204,62 @@ class Engine:
         self.launches += sum(1 for p in passes if p.ops)
 
     def apply_ops(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
-        """Apply unitary ops (no measure/reset/perm) in order."""
+        """Apply unitary ops (no measure/reset/perm) in order.
+
+        The first time an op sequence is applied, each pass is launched as soon
+        as it is planned (the GPU works on it while the host plans the next
+        one), and the plan is kept as a program: its passes grouped into
+        segments with their packed qs_pass / qs_op arrays and matrix tables.
+        Applying the same sequence again (same ops and matrices, qubit count,
+        precision and knobs) replays the program: one table upload and one
+        library call per segment, no lowering or planning."""
         if not self.fusion:
             for op in ops:
                 self.apply_single(vec, n, op)
             return
-        # each pass is launched as soon as it is planned: the GPU works on it
-        # while the host plans the next one
+        key = self._program_key(vec, n, ops)
+        prog = self.programs.get(key) if key is not None else None
+        if prog is not None:
+            self.programs.move_to_end(key)
+            self._run_program(vec, n, prog)
+            return
+        steps = []
         for step in self.plan_iter(vec, n, ops):
             if isinstance(step, Pass):
                 self.run_passes(vec, n, [step])
             else:
                 self.apply_single(vec, n, step.op)
+            steps.append(step)
+        if key is not None:
+            self.programs[key] = _Program(steps, vec.dtype)
+            while len(self.programs) > self.max_programs:
+                self.programs.popitem(last=False)
+
+    def _program_key(self, vec: torch.Tensor, n: int, ops: Sequence[Op]):
+        """Exact key of an op sequence (None: not kept, e.g. batched or tagged ops)."""
+        if not ops:
+            return None
+        parts = [n, str(vec.dtype), self.knobs(vec, n)]
+        for op in ops:
+            if op.batch is not None or op.tag is not None or op.kind not in ("mat", "diag", "antidiag", "swap"):
+                return None
+            parts.append((op.kind, op.tbits, op.cbits, op.mat.tobytes()))
+        return tuple(parts)
+
+    def _run_program(self, vec: torch.Tensor, n: int, prog: "_Program"):
+        st = self.stream
+        for seg in prog.segments:
+            if seg[0] == "single":
+                self.apply_single(vec, n, seg[1])
+                continue
+            _, cps, npass, cops, nops, host, pinned = seg
+            mats = torch.empty(pinned.shape, dtype=pinned.dtype, device=self.device)
+            mats.copy_(pinned, non_blocking=True)
+            self.h2d_bytes += mats.numel() * mats.element_size()
+            N.call("qs_apply_fused_ex", C.c_void_p(vec.data_ptr()), n, qs_dtype(vec), cps, npass, cops, nops,
+                   C.c_void_p(mats.data_ptr()), C.c_void_p(host.ctypes.data), int(mats.numel()), st)
+            self.launches += npass
+            self._keep = mats
 
     # ---- reductions / measurement -------------------------------------------------------
     def prob0(self, src: torch.Tensor, n: int, bit: int, src_kind: int = N.QS_SRC_SV) -> float:

@@ -222,8 +222,8 @@ def matrix_instr(u: np.ndarray) -> float:
     cheap = nz & ~unit & ((u.imag == 0) | (u.real == 0))
     general = nz & ~unit & ~cheap
     per_row = 4 * general.sum(axis=1) + 2 * cheap.sum(axis=1) + 2 * unit.sum(axis=1)
-    first_unit = np.array([bool(unit[r, np.flatnonzero(nz[r])[0]]) if nz[r].any() else False
-                           for r in range(u.shape[0])])
+    first = np.argmax(nz, axis=1)  # column of each row's first nonzero entry
+    first_unit = unit[np.arange(u.shape[0]), first] & nz.any(axis=1)
     per_row = per_row - 2 * first_unit
     return float(per_row.mean())
 

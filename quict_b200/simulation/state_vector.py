@@ -94,6 +94,7 @@ class StateVectorSimulator:
         self._qubits = 0
         self._vector: Optional[torch.Tensor] = None
         self.last_sample_indices: Optional[torch.Tensor] = None
+        self._lowered: dict = {}  # circuit key -> lowered ops (recent circuits)
 
     # ---- reference properties ---------------------------------------------------------
     @property
@@ -166,6 +167,22 @@ class StateVectorSimulator:
 
     def _run_gates(self, gates: List):
         n = self._qubits
+        # a circuit of plain gates seen before is not lowered again (the
+        # engine then replays its planned program as well)
+        key = _circuit_key(gates, n, self._legacy)
+        if key is not None:
+            ops = self._lowered.get(key)
+            if ops is None:
+                ops = [op for g in gates for op in lower_gate(g, n, self._legacy)]
+                if any(op.kind in ("measure", "reset", "perm") for op in ops):
+                    ops = None
+                else:
+                    self._lowered[key] = ops
+                    while len(self._lowered) > 8:
+                        self._lowered.pop(next(iter(self._lowered)))
+            if ops is not None:
+                self._engine.apply_ops(self._vector, n, ops)
+                return
         pending: List[Op] = []
         idx = 0
         while idx < len(gates):
@@ -299,6 +316,34 @@ class MeasuredProb(float):
 
     def get(self) -> float:
         return float(self)
+
+
+# gate types whose matrix follows from the type, the qubit count and pargs
+_PARAM_DETERMINED = None
+
+
+def _circuit_key(gates, n: int, legacy: bool):
+    """Exact key of a list of plain gates (None when it holds anything else:
+    triggers, measurements, operators): per gate its type, qubits, parameters
+    and precision, plus the matrix itself for custom-matrix gates."""
+    global _PARAM_DETERMINED
+    if _PARAM_DETERMINED is None:
+        from ..core.gate import GATE_BY_NAME
+        _PARAM_DETERMINED = frozenset(GATE_BY_NAME) - {"unitary", "measure", "reset", "barrier"}
+    parts = [n, legacy]
+    for g in gates:
+        t = getattr(g, "type", None)
+        name = getattr(t, "name", None)
+        if name is None or name in ("measure", "reset") or _is_trigger(g):
+            return None
+        k = (name, tuple(g.cargs), tuple(g.targs), tuple(g.pargs), str(getattr(g, "precision", "")))
+        if name not in _PARAM_DETERMINED:
+            m = g.matrix
+            if m is None:
+                return None
+            k = k + (np.asarray(m).tobytes(),)
+        parts.append(k)
+    return tuple(parts)
 
 
 def _is_trigger(g) -> bool:
