@@ -169,6 +169,69 @@ k_diag_v2(float2* __restrict__ v, uint64_t items2, Plan plan, uint64_t fixed, in
     }
 }
 
+// complex64, target bit < 5: each lane moves a float4 (amplitudes 2l, 2l+1
+// of a 64-amplitude chunk); the partner of bit 0 is the lane's other half,
+// the partner of bit b >= 1 sits in lane l ^ 2^(b-1).  Control bits 0..5 are
+// checked per amplitude (cmask_lo), higher ones are fixed by the chunk plan.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_1q_shfl_v2(float2* __restrict__ v, uint64_t chunks, Plan plan_hi, uint64_t cmask_hi, uint32_t cmask_lo, int bit,
+             Mat<float2, 4> M) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (kThreads / 32);
+    const uint64_t w0 = uint64_t(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+    float4* __restrict__ v4 = reinterpret_cast<float4*>(v);
+    const bool one = bit > 0 && ((lane >> (bit - 1)) & 1);
+    const bool act0 = (uint32_t(2 * lane) & cmask_lo) == cmask_lo;
+    const bool act1 = (uint32_t(2 * lane + 1) & cmask_lo) == cmask_lo;
+    for (uint64_t c0 = w0; c0 < chunks; c0 += warps * kUnroll) {
+        float4 a[kUnroll];
+        uint64_t q[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c < chunks) {  // warp-uniform
+                q[u] = ((expand(c << 6, plan_hi) | cmask_hi) >> 1) + lane;
+                a[u] = v4[q[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c >= chunks) continue;
+            const float2 x0 = make_float2(a[u].x, a[u].y), x1 = make_float2(a[u].z, a[u].w);
+            float2 y0, y1;
+            if (bit == 0) {
+                if (KIND == QS_K_DENSE) {
+                    y0 = cfma(M.m[0], x0, cmul(M.m[1], x1));
+                    y1 = cfma(M.m[2], x0, cmul(M.m[3], x1));
+                } else {
+                    y0 = cmul(M.m[1], x1);
+                    y1 = cmul(M.m[2], x0);
+                }
+            } else {
+                const int pm = 1 << (bit - 1);
+                float4 pa;
+                pa.x = __shfl_xor_sync(0xffffffffu, a[u].x, pm);
+                pa.y = __shfl_xor_sync(0xffffffffu, a[u].y, pm);
+                pa.z = __shfl_xor_sync(0xffffffffu, a[u].z, pm);
+                pa.w = __shfl_xor_sync(0xffffffffu, a[u].w, pm);
+                const float2 p0 = make_float2(pa.x, pa.y), p1 = make_float2(pa.z, pa.w);
+                if (KIND == QS_K_DENSE) {
+                    y0 = one ? cfma(M.m[2], p0, cmul(M.m[3], x0)) : cfma(M.m[0], x0, cmul(M.m[1], p0));
+                    y1 = one ? cfma(M.m[2], p1, cmul(M.m[3], x1)) : cfma(M.m[0], x1, cmul(M.m[1], p1));
+                } else {
+                    y0 = one ? cmul(M.m[2], p0) : cmul(M.m[1], p0);
+                    y1 = one ? cmul(M.m[2], p1) : cmul(M.m[1], p1);
+                }
+            }
+            if (!act0) y0 = x0;
+            if (!act1) y1 = x1;
+            if (act0 || act1) v4[q[u]] = make_float4(y0.x, y0.y, y1.x, y1.y);
+        }
+    }
+}
+
 // ------------------------------------------------------------ 1q, shuffles
 // Target bit < 5 and n >= 5.  Each warp owns 32 consecutive amplitudes of the
 // compact space (control bits >= 5 removed); lane partner = lane ^ (1<<bit).
@@ -402,6 +465,22 @@ int apply_1q_t(void* vec, int n, int bit, uint64_t cmask, int kind, const double
         launch_diag<V>(v, items, p, fixed, -1, bit, D, st);
         QS_CHECK_LAUNCH("qs_apply_1q(diag)");
         return QS_OK;
+    }
+    if constexpr (sizeof(V) == 8) {
+        if (bit < 5 && n >= 6) {  // 64-amplitude chunks, float4 per lane
+            const uint64_t chi = cmask & ~uint64_t(63);
+            Plan p = make_plan(chi);
+            uint64_t chunks = (uint64_t(1) << (n - p.nb)) >> 6;
+            unsigned grid = grid_for(chunks, (kThreads / 32) * kUnroll, 8);
+            if (kind == QS_K_DENSE)
+                k_1q_shfl_v2<QS_K_DENSE><<<grid, kThreads, 0, st>>>((float2*)v, chunks, p, chi, uint32_t(cmask & 63),
+                                                                    bit, M);
+            else
+                k_1q_shfl_v2<QS_K_ANTIDIAG><<<grid, kThreads, 0, st>>>((float2*)v, chunks, p, chi,
+                                                                       uint32_t(cmask & 63), bit, M);
+            QS_CHECK_LAUNCH("qs_apply_1q(shfl, float4)");
+            return QS_OK;
+        }
     }
     const uint64_t cmask_hi = cmask & ~uint64_t(31);
     if (bit < 5 && n >= 5) {

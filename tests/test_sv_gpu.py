@@ -106,8 +106,9 @@ def test_every_gate_every_placement_vs_oracle(cuda_ok, n, tile):
     for fusion in (True, False):
         v = sim(fusion=fusion, tile_bits=tile[0], low_bits=tile[1]).run(build_circuit(gl, n)).get()
         np.testing.assert_allclose(v, ref, rtol=0, atol=1e-12)
-    v = sim("single", tile_bits=tile[0], low_bits=tile[1]).run(build_circuit(gl, n, "single")).get()
-    np.testing.assert_allclose(v, ref, rtol=0, atol=1e-5)
+        # complex64 single-gate kernels move two adjacent amplitudes per 128-bit access
+        v = sim("single", fusion=fusion, tile_bits=tile[0], low_bits=tile[1]).run(build_circuit(gl, n, "single")).get()
+        np.testing.assert_allclose(v, ref, rtol=0, atol=1e-5)
 
 
 def test_config0_20q_200_gates(cuda_ok):
