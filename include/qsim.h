@@ -252,7 +252,9 @@ int qs_apply_pauli_sum(const void* psi, void* out, int n, int dtype, const uint6
                        const uint64_t* zmask, const double* coeff, int nterms, void* stream);
 
 /* out_dev[2*i] + i*out_dev[2*i+1] = sum over instance i of conj(a_j) b_j
- * (FP64), instances of 2^inst_bits amplitudes.  ws: qs_reduce_ws_bytes. */
+ * (FP64), instances of 2^inst_bits amplitudes.  ws: at least 16 bytes per
+ * instance; a larger workspace (up to 16 KiB per instance) lets each
+ * instance use more thread blocks (partial sums). */
 int qs_inner_batched(const void* a, const void* b, int n, int dtype, int inst_bits, double* out_dev,
                      void* ws, size_t ws_bytes, void* stream);
 

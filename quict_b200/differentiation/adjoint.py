@@ -278,7 +278,7 @@ class BatchedAdjoint:
                qs_dtype(psi), x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
                c.ctypes.data_as(C.c_void_p), len(x), self.stream)
         e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
-        ws = self.ws.get(16 * bp * 64 + 256)
+        ws = self.ws.get(16 * bp * 1024 + 256)  # qs_inner_batched: up to 1024 partials per instance
         N.call("qs_inner_batched", C.c_void_p(psi.data_ptr()), C.c_void_p(lam.data_ptr()), nbits, qs_dtype(psi),
                self.n, C.c_void_p(e.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(), self.stream)
         self.launches += 2
@@ -332,7 +332,7 @@ class BatchedAdjoint:
         gp.partials = torch.empty(2 * gp.nslots * bp * gp.tiles_per_inst, dtype=torch.float64, device=self.dev)
         gp.sums = torch.empty(2 * gp.nslots * bp, dtype=torch.float64, device=self.dev)
         gp.e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
-        gp.ws = torch.empty(16 * bp * 64 + 256, dtype=torch.uint8, device=self.dev)
+        gp.ws = torch.empty(16 * bp * 1024 + 256, dtype=torch.uint8, device=self.dev)
         # gradient = W @ Im<lam|G|psi>, W[param, slot] = scale: a fixed-order (deterministic)
         # sum over the gates that share a parameter
         w = np.zeros((self.circuit.num_params, gp.nslots))

@@ -12,11 +12,12 @@ large ones (2^24) use the whole GPU.
 """
 from __future__ import annotations
 
-from typing import List, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
 
+from ..simulation.autotune import Autotuner, tune_key
 from .adjoint import BatchedAdjoint, GradientPlan
 from .circuit import maxcut_observable, qaoa_circuit, random_regular_graph
 
@@ -36,17 +37,51 @@ def qaoa_instances(count: int = 512, sizes: Sequence[int] = tuple(range(10, 25, 
     return out
 
 
+def _tile_maker(n, edges, p, precision, device_id, jit):
+    def make(fk, pk):
+        return BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id,
+                              tile_bits=fk, pair_tile_bits=pk, jit=jit)
+    make.precision, make.n = precision, n
+    return make
+
+
+def tune_qaoa_size(tuner: Autotuner, n: int, precision: str, device_id: int = 0, seed: int = 11):
+    """Tune the forward / pair tile widths of n-qubit MaxCut QAOA gradients
+    (a seeded depth-6 instance) and store them under kind "qaoa"."""
+    (nn, edges, p, prm), = qaoa_instances(1, sizes=(n,), depths=(6, 6), seed=seed)
+    dev = torch.device("cuda", device_id)
+    key = tune_key(torch.cuda.get_device_name(dev), 8 if precision == "single" else 16, n, "qaoa")
+    return tuner.tune_adjoint(_tile_maker(n, edges, p, precision, device_id, True), np.asarray(prm)[None, :], key)
+
+
 class UnevenQAOABatch:
     """`jit_min_qubits`: instances of at least that many qubits run their
     register passes as run-time compiled kernels (their kernels dominate the
     replay); smaller ones keep the generic kernels, whose per-instance
-    compilation would not pay off."""
+    compilation would not pay off.  Tile widths come per qubit count from the
+    autotuner's "qaoa" entries (`autotune=True` tunes sizes it has none for,
+    on the first instance of that size)."""
 
     def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16,
-                 jit_min_qubits: int = 22):
+                 jit_min_qubits: int = 22, autotune: bool = False, tuner: Optional[Autotuner] = None):
         self.instances = instances
         self.jit_min_qubits = jit_min_qubits
+        tuner = tuner or Autotuner()
+        dev = torch.device("cuda", device_id)
+        esize = 8 if precision == "single" else 16
+        self.tiles = {}  # n -> (forward tile bits, pair tile bits) or None (engine defaults)
+        for n, edges, p, prm in instances:
+            if n in self.tiles:
+                continue
+            key = tune_key(torch.cuda.get_device_name(dev), esize, n, "qaoa")
+            kn = tuner.lookup_adjoint(key)
+            if kn is None and autotune:
+                kn, _, _ = tuner.tune_adjoint(_tile_maker(n, edges, p, precision, device_id, n >= jit_min_qubits),
+                                              np.asarray(prm)[None, :], key)
+            self.tiles[n] = kn
         self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision, device_id,
+                                       tile_bits=self.tiles[n][0] if self.tiles[n] else None,
+                                       pair_tile_bits=self.tiles[n][1] if self.tiles[n] else None,
                                        jit=n >= jit_min_qubits)
                         for n, edges, p, _ in instances]
         self.captured_launches = 0  # kernel launches recorded in the graph

@@ -26,7 +26,7 @@ import math
 import os
 import time
 from dataclasses import asdict, dataclass, field
-from typing import Callable, Dict, List, Optional, Sequence
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 PACKAGED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
 
@@ -68,6 +68,17 @@ def candidates(esize: int, n: int) -> List[Knobs]:
                 if k <= n and nlow <= k:
                     out.append(Knobs(k, nlow, mb))
     return out
+
+
+def adjoint_candidates(precision: str, n: int) -> List[Tuple[int, int]]:
+    """(forward tile bits, pair tile bits) for an n-qubit adjoint gradient: the
+    register tiles from the smallest (64-thread CTAs) to 64 KiB; a pair tile
+    holds the psi/lam bit besides n qubit bits."""
+    k0 = 12 if precision == "double" else 13
+    min_k = 9 if precision == "double" else 10
+    fwd = sorted({k for k in (min_k, min_k + 1, k0 - 1) if k <= n}) or [min(min_k, n)]
+    pair = [k for k in range(min_k, k0 + 1) if k <= n + 1]
+    return [(f, p) for f in fwd for p in pair]
 
 
 def tune_key(device_name: str, esize: int, n: int, kind: str) -> str:
@@ -118,6 +129,53 @@ class Autotuner:
         with open(tmp, "w") as f:
             json.dump(d, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
+
+    def lookup_adjoint(self, key: str) -> Optional[Tuple[int, int]]:
+        """(forward tile bits, pair tile bits) of an adjoint-gradient entry."""
+        for path in (self.cache_path, self.packaged_path):
+            e = _load(path).get(key)
+            if e is not None and "pair_tile_bits" in e.get("knobs", {}):
+                return int(e["knobs"]["tile_bits"]), int(e["knobs"]["pair_tile_bits"])
+        return None
+
+    def tune_adjoint(self, make_engine: Callable[[int, int], object], params, key: str, reps: int = 3,
+                     store: bool = True) -> Tuple[Tuple[int, int], float, Dict[str, float]]:
+        """Time every (forward tile, pair tile) candidate of an adjoint
+        gradient on `params` (``adjoint_candidates``), each after its generated
+        kernels are compiled; store and return the fastest."""
+        import torch
+
+        from .. import _native as N
+        trials: Dict[str, float] = {}
+        best, best_ms = None, math.inf
+        for fk, pk in adjoint_candidates(make_engine.precision, make_engine.n):
+            eng = make_engine(fk, pk)
+            gp = eng.plan_gradient(params)
+            eng.launch(gp)
+            N.jit_wait(600)
+            eng.launch(gp)
+            torch.cuda.synchronize(eng.dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                eng.launch(gp)
+            b.record()
+            torch.cuda.synchronize(eng.dev)
+            t = a.elapsed_time(b) / reps
+            trials[f"tile_bits={fk} pair_tile_bits={pk}"] = t
+            if t < best_ms:
+                best, best_ms = (fk, pk), t
+            del gp, eng
+        if store:
+            d = _load(self.cache_path)
+            d[key] = {"knobs": {"tile_bits": best[0], "pair_tile_bits": best[1]}, "ms": best_ms, "trials": trials,
+                      "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
+            os.makedirs(os.path.dirname(os.path.abspath(self.cache_path)), exist_ok=True)
+            tmp = self.cache_path + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(d, f, indent=1, sort_keys=True)
+            os.replace(tmp, self.cache_path)
+        return best, best_ms, trials
 
     # ---- search ------------------------------------------------------------------
     @staticmethod
@@ -195,9 +253,19 @@ def main() -> None:
     ap.add_argument("--precision", nargs="+", default=["double", "single"])
     ap.add_argument("--gates", type=int, default=1000)
     ap.add_argument("--out", default=None, help="cache file (default: the user cache)")
+    ap.add_argument("--qaoa", action="store_true",
+                    help="tune the adjoint-gradient tiles of seeded MaxCut QAOA instances (depth 6) instead")
     a = ap.parse_args()
     dev = torch.device("cuda", 0)
     tuner = Autotuner(cache_path=a.out)
+    if a.qaoa:
+        from ..differentiation.qaoa import tune_qaoa_size
+        for n in a.qubits:
+            for prec in a.precision:
+                (fk, pk), ms, _ = tune_qaoa_size(tuner, n, prec)
+                print(json.dumps({"n": n, "precision": prec, "tile_bits": fk, "pair_tile_bits": pk, "ms": ms}),
+                      flush=True)
+        return
     for n in a.qubits:
         for prec in a.precision:
             dt = torch.complex128 if prec == "double" else torch.complex64

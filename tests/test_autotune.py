@@ -71,3 +71,23 @@ def test_autotuned_run_matches_oracle(cuda_ok, tmp_path, monkeypatch):
     v2 = sim2.run(c).get()
     np.testing.assert_allclose(v2, v, atol=1e-12)
     assert sim2.engine.knobs(sim2._vector, n) == Knobs.from_json(d[key]["knobs"])
+
+
+def test_adjoint_candidates_and_cache_lookup(tmp_path):
+    """Adjoint tile candidates stay inside the register-tile range and the
+    pair tile fits the psi/lam vector; "qaoa" entries read back as (forward,
+    pair) tile widths and are not mistaken for fused-pass knobs."""
+    import json
+    from quict_b200.simulation.autotune import Autotuner, adjoint_candidates
+    for prec, lo, hi in (("single", 10, 13), ("double", 9, 12)):
+        for n in (10, 12, 16, 24):
+            c = adjoint_candidates(prec, n)
+            assert c and all(lo <= f <= max(lo, min(hi - 1, n)) and lo <= p <= min(hi, n + 1) for f, p in c)
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"dev|c64|n16|qaoa": {"knobs": {"tile_bits": 11, "pair_tile_bits": 12}, "ms": 1.0},
+                                "dev|c64|n16|sv": {"knobs": {"tile_bits": 11, "low_bits": 5, "merge_bits": 2,
+                                                             "max_pass_cost": None}, "ms": 1.0}}))
+    t = Autotuner(cache_path=str(path), packaged_path=str(tmp_path / "none.json"))
+    assert t.lookup_adjoint("dev|c64|n16|qaoa") == (11, 12)
+    assert t.lookup_adjoint("dev|c64|n16|sv") is None
+    assert t.lookup_adjoint("dev|c64|n18|qaoa") is None
