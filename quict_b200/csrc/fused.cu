@@ -1505,10 +1505,11 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     put64(o_misc, ~a.pairmask);
     put64(o_misc + 8, uint64_t(a.inst_shift));
     // value class of a matrix entry: 0, 1, -1, general (3), real (4), imaginary
-    // (5); entries of per-instance tables are general
-    auto vclass = [&](int o, int idx) -> int {
-        if (strided[o]) return 3;
-        const V v = pm[idx];
+    // (5).  An entry of a per-instance table gets the class that holds for
+    // every instance's value (e.g. real for the entries of Ry tables, imaginary
+    // for the off-diagonal entries of Rx tables); the value itself is read from
+    // the staged table at run time.
+    auto value_class = [](const V v) -> int {
         if (v.y == 0) {
             if (v.x == 0) return 0;
             if (v.x == 1) return 1;
@@ -1517,6 +1518,36 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
         }
         return v.x == 0 ? 5 : 3;
     };
+    auto join_class = [](int c1, int c2) -> int {
+        if (c1 == c2) return c1;
+        const bool r1 = c1 == 0 || c1 == 1 || c1 == 2 || c1 == 4, r2 = c2 == 0 || c2 == 1 || c2 == 2 || c2 == 4;
+        if (r1 && r2) return 4;
+        if ((c1 == 0 || c1 == 5) && (c2 == 0 || c2 == 5)) return 5;
+        return 3;
+    };
+    // instances of a batched pass: the vector bits above inst_shift, less the pair bit
+    const int64_t ninst =
+        batched && a.inst_shift > 0 ? (int64_t(1) << (a.n - a.inst_shift - (a.pairmask ? 1 : 0))) : int64_t(1);
+    std::vector<uint8_t> scls(size_t(NM), 3);
+    for (int o = 0; o < a.nops; ++o) {
+        if (!strided[o]) continue;
+        const KCopy& c = a.cp[o];
+        const int D = 1 << c.m;
+        const int cnt = c.diag ? D : D * D;
+        for (int e = 0; e < cnt; ++e) {
+            const int kr = c.diag ? e : e / D, kc = c.diag ? 0 : e % D;
+            int sr = 0, sc = 0;
+            for (int i = 0; i < c.m; ++i) {
+                sr |= ((kr >> i) & 1) << c.perm[i];
+                sc |= ((kc >> i) & 1) << c.perm[i];
+            }
+            const int64_t src = c.goff + (c.diag ? sr : sr * D + sc);
+            int cl = value_class(hm[src]);
+            for (int64_t i = 1; i < ninst && cl != 3; ++i) cl = join_class(cl, value_class(hm[src + i * c.stride]));
+            scls[size_t(c.soff + e)] = uint8_t(cl);
+        }
+    }
+    auto vclass = [&](int o, int idx) -> int { return strided[o] ? int(scls[size_t(idx)]) : value_class(pm[idx]); };
     auto mref = [&](int o, int idx) -> std::string {
         return (strided[o] ? "msm[" : "p.m[") + std::to_string(idx) + "]";
     };
@@ -1526,11 +1557,32 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
         const int cnt = c.diag ? (1 << c.m) : (1 << (2 * c.m));
         for (int e = 0; e < cnt; ++e) out.classes[c.soff + e] = uint8_t(vclass(o, c.soff + e));
     }
+    // Diagonal tables indexed by thread bits (a different entry per lane) are
+    // copied to shared memory once per CTA: parameter-space loads with lane-
+    // dependent addresses are serialised, shared-memory loads are not.
+    std::vector<int> doff(size_t(NOPS), -1);
+    int ndsm = 0;
+    for (int o = 0; o < a.nops; ++o) {
+        const KOp& op = a.ops[o];
+        const bool dg = op.code == QS_OP_DIAG || (op.code == QS_OP_EXPECT && (op.flags & QS_OPF_DIAG));
+        if (!dg || op.nh == 0 || strided[o]) continue;
+        bool thr = false;
+        for (int q = 0; q < op.nh; ++q) thr = thr || op.hsrc[q] < 64;
+        if (!thr) continue;
+        doff[size_t(o)] = ndsm;
+        ndsm += 1 << a.cp[o].m;
+    }
+    // the table of a diagonal with other-bit index h, as an expression prefix
+    auto dtab = [&](int o) -> std::string {
+        if (strided[o]) return "msm[" + std::to_string(int(a.ops[o].moff)) + " + ";
+        if (doff[size_t(o)] >= 0) return "dsm[" + std::to_string(doff[size_t(o)]) + " + ";
+        return "p.m[" + std::to_string(int(a.ops[o].moff)) + " + ";
+    };
     const unsigned hoff_n = (1u << H) < 2u ? 2u : (1u << H);  // a 16-byte multiple
     out.threads = threads;
     out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * size_t(hoff_n) +
                (a.nexp > 0 ? sizeof(double2) * size_t(nwarps) * size_t(a.nexp) : 0) +
-               (batched ? sizeof(V) * size_t(NM) : 0);
+               (batched ? sizeof(V) * size_t(NM) : 0) + sizeof(V) * size_t(ndsm);
     if (!with_source) return true;
     const char* VT = C128 ? "double2" : "float2";
     const char* ST = C128 ? "double" : "float";
@@ -1573,9 +1625,14 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
     g.add("  double2* const ered = reinterpret_cast<double2*>(hoff + %du);\n", hoff_n);
     g.add("  V* const msm = reinterpret_cast<V*>(ered + %d);\n", a.nexp > 0 ? nwarps * a.nexp : 0);
+    g.add("  V* const dsm = msm + %d;\n", batched ? NM : 0);
     g.add("  const u32 tid = threadIdx.x;\n");
     g.add("  for (u32 j = tid; j < %du; j += %du) { u64 o = 0;\n", 1u << H, threads);
     g.add("#pragma unroll\n    for (int t = 0; t < %d; ++t) if ((j >> t) & 1u) o |= p.hibit[t];\n    hoff[j] = o; }\n", H);
+    for (int o = 0; o < a.nops; ++o)
+        if (doff[size_t(o)] >= 0)
+            g.add("  for (u32 q = tid; q < %du; q += %du) dsm[%d + q] = p.m[%d + q];\n", 1u << a.cp[o].m,
+                  unsigned(threads), doff[size_t(o)], int(a.ops[o].moff));
     g.add("  u64 gthr = 0;\n");
     for (int i = 0; i < nT; ++i) g.add("  if ((tid >> %d) & 1u) gthr |= p.gthr[%d];\n", i, i);
     for (int si = 0; si < a.nstages; ++si) {
@@ -1754,8 +1811,7 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
                         else if (cl == 5) e = "imul(" + mref(o, idx) + ".y, " + vname(var[s]) + ")";
                         else e = "cmul(" + vname(var[s]) + ", " + mref(o, idx) + ")";
                     } else {
-                        e = "cmul(" + vname(var[s]) + ", " + std::string(strided[o] ? "msm[" : "p.m[") +
-                            std::to_string(int(op.moff)) + " + ((h" + std::to_string(o) + " << " +
+                        e = "cmul(" + vname(var[s]) + ", " + dtab(o) + "((h" + std::to_string(o) + " << " +
                             std::to_string(int(op.ns)) + ") | " + std::to_string(k) + "u)])";
                     }
                     const int nid = fresh++;
@@ -1775,10 +1831,9 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
                     for (int s = 0; s < E; s += 2) {
                         const int k = op.kidx[s];
                         std::string d = op.nh == 0 ? mref(o, op.moff + k)
-                                                   : std::string(strided[o] ? "msm[" : "p.m[") +
-                                                         std::to_string(int(op.moff)) + " + ((h" + std::to_string(o) +
-                                                         " << " + std::to_string(int(op.ns)) + ") | " +
-                                                         std::to_string(k) + "u)]";
+                                                   : dtab(o) + "((h" + std::to_string(o) + " << " +
+                                                         std::to_string(int(op.ns)) + ") | " + std::to_string(k) +
+                                                         "u)]";
                         g.s += "      { const V acc = cmul(" + d + ", " + vname(var[s]) + "); const V l = " +
                                vname(var[s | 1]) + ";\n";
                         g.s += "        pr += l.x * acc.x + l.y * acc.y; pi += l.x * acc.y - l.y * acc.x; }\n";
