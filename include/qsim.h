@@ -261,6 +261,71 @@ int qs_inner_batched(const void* a, const void* b, int n, int dtype, int inst_bi
 /* out[s] = sum_{t < seglen} in[s * seglen + t] for complex FP64 pairs. */
 int qs_segment_sum(const double* in_dev, int64_t nseg, int64_t seglen, double* out_dev, void* stream);
 
+/* ---- persistent batch: many problems in one launch ------------------------- */
+/* One problem of a batch: an n-qubit circuit from |0...0>, its observable H
+ * and the adjoint sweep of its gradient.  Passes, ops, matrices, observable
+ * terms and weights index arrays shared by the whole batch. */
+typedef struct qs_batch_inst {
+  int32_t n;           /* qubits; psi has 2^n amplitudes                       */
+  int32_t fwd_begin;   /* forward passes[fwd_begin, +nfwd) over n bits; the    */
+  int32_t nfwd;        /*   first reads |0...0> (>= 1 pass)                    */
+  int32_t bwd_begin;   /* backward pair passes[bwd_begin, +nbwd) over n + 1    */
+  int32_t nbwd;        /*   bits, pair = n + 1 (psi / lam on vector bit n)      */
+  int32_t term_begin;  /* H = sum of terms [term_begin, +nterms) (1..128) of    */
+  int32_t nterms;      /*   xmask / zmask / coeff (as qs_apply_pauli_sum)       */
+  int32_t nslots;      /* EXPECT slots of the backward passes                  */
+  int32_t nparams;     /* gradient length                                       */
+  int32_t pad;
+  int64_t w_begin;     /* W = weights[w_begin, +nparams*nslots), row-major:    */
+                       /*   gradient = W Im(per-slot sums of <lam|G|psi>)       */
+} qs_batch_inst;
+
+/* What a planned batch needs (filled by qs_batch_plan). */
+typedef struct qs_batch_sizes {
+  int64_t blob_bytes;       /* the plan (copy it to the device unchanged)       */
+  int64_t state_elems;      /* state pool: complex elements (sum of 2^(n+1))    */
+  int64_t partial_doubles;  /* partials pool                                     */
+  int64_t grad_doubles;     /* gradient output: instances' gradients in order   */
+  int64_t energy_doubles;   /* energy output: (re, im) per instance             */
+  int64_t ctrl_bytes;       /* control words                                     */
+  int64_t smem_bytes;       /* dynamic shared memory per CTA                     */
+  int32_t threads;          /* CTA size                                          */
+  int32_t nitems;           /* work items                                        */
+  int32_t nstages;          /* register stages over all instances                */
+  int32_t big;              /* some pass needs the wide dense-op code paths      */
+  int32_t dtype;
+  int32_t pad;
+} qs_batch_sizes;
+
+/* Plan a batch on the host.  Every stage of every problem (register passes,
+ * lam = H psi with the energy partials, the final reduction) is cut into
+ * work items of `tiles_per_item` tiles / `amps_per_ham_item` amplitudes.
+ * blob == NULL: only fill *sizes (and state_off[i], the element offset of
+ * problem i's pair vector in the state pool, if state_off != NULL); else
+ * write the plan (blob_bytes >= sizes->blob_bytes).  Passes follow the rules
+ * of qs_apply_fused / qs_adjoint_pair and must be register tiles (k in
+ * [9, 12] complex128 / [10, 13] complex64, nlow >= 5); a problem's backward
+ * passes share one k.  No reference counterpart (the reference has neither
+ * gradients nor batching). */
+int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, const qs_pass* passes, int npasses,
+                  const qs_op* ops, int64_t nops, int64_t mats_count, const uint64_t* xmask,
+                  const uint64_t* zmask, const double* coeff, int nterms_total, const double* weights,
+                  int64_t nweights, int64_t tiles_per_item, int64_t amps_per_ham_item, void* blob,
+                  size_t blob_bytes, qs_batch_sizes* sizes, int64_t* state_off);
+
+/* Run a planned batch as ONE persistent kernel launch (after a memset of the
+ * control words, both on `stream`).  blob_dev: the plan in device memory
+ * (16-byte aligned); states: the state pool; mats: the matrix table the ops
+ * index (mats_count entries, the state's dtype); partials, energies (re, im
+ * per problem), grads: outputs sized by qs_batch_plan; ctrl: ctrl_bytes of
+ * device memory.  Work items wait for their problem's earlier stages with a
+ * bounded wait of timeout_s seconds; a wait that gives up stores
+ * (1 << 32) | item in control word 1 (bytes 8..15 of ctrl, 0 on success) and
+ * the launch ends early.  Replaces nothing in the reference (see above). */
+int qs_batch_launch(const qs_batch_sizes* sizes, const void* blob_dev, void* states, const void* mats,
+                    double* partials, double* energies, double* grads, void* ctrl, size_t ctrl_bytes,
+                    double timeout_s, void* stream);
+
 /* ---- measurement, reset, sampling ------------------------------------------ */
 size_t qs_reduce_ws_bytes(int n);
 /* *out_dev <- sum over {i : bit b of i is 0} of p_i, in FP64 (src = QS_SRC_*).

@@ -74,7 +74,42 @@ class qs_pass(C.Structure):
     ]
 
 
+class qs_batch_inst(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("fwd_begin", C.c_int32),
+        ("nfwd", C.c_int32),
+        ("bwd_begin", C.c_int32),
+        ("nbwd", C.c_int32),
+        ("term_begin", C.c_int32),
+        ("nterms", C.c_int32),
+        ("nslots", C.c_int32),
+        ("nparams", C.c_int32),
+        ("pad", C.c_int32),
+        ("w_begin", C.c_int64),
+    ]
+
+
+class qs_batch_sizes(C.Structure):
+    _fields_ = [
+        ("blob_bytes", C.c_int64),
+        ("state_elems", C.c_int64),
+        ("partial_doubles", C.c_int64),
+        ("grad_doubles", C.c_int64),
+        ("energy_doubles", C.c_int64),
+        ("ctrl_bytes", C.c_int64),
+        ("smem_bytes", C.c_int64),
+        ("threads", C.c_int32),
+        ("nitems", C.c_int32),
+        ("nstages", C.c_int32),
+        ("big", C.c_int32),
+        ("dtype", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
 assert C.sizeof(qs_op) == 80
+assert C.sizeof(qs_batch_inst) == 48 and C.sizeof(qs_batch_sizes) == 80
 assert C.sizeof(qs_pass) == 8 + 4 * QS_MAX_TILE_BITS + 16
 
 _vp, _i, _i64, _u64, _d, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
@@ -111,6 +146,10 @@ SIGNATURES = {
     "qs_apply_fused_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp]),
     "qs_adjoint_pair_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp,
                                 _i64, _vp]),
+    "qs_batch_plan": (_i, [_i, C.POINTER(qs_batch_inst), _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _i64,
+                           _vp, _vp, _vp, _i, _vp, _i64, _i64, _i64, _vp, _sz, C.POINTER(qs_batch_sizes),
+                           C.POINTER(C.c_int64)]),
+    "qs_batch_launch": (_i, [C.POINTER(qs_batch_sizes), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _d, _vp]),
     "qs_jit_shutdown": (_i, []),
     "qs_jit_set_mode": (_i, [_i]),
     "qs_jit_wait": (_i, [_d]),

@@ -299,16 +299,8 @@ class BatchedAdjoint:
         p, b, bp = self._prepare(params)
         nbits = self.n + (bp.bit_length() - 1)
         gp = GradientPlan(b=b, bp=bp, nbits=nbits)
-        gp.fwd = self._build(nbits, [op for _, op in self._gate_ops(p, False)], adjoint=False)
-        inv = self._gate_ops(p, True)
-        slot_of = {u: s for s, u in enumerate(self._param_units)}
-        ops: List[Op] = []
-        for ui, op in reversed(inv):
-            un = self._units[ui]
-            if un.fixed is None:
-                ops.append(Op("expect", op.tbits, (), un.gen, tag=("expect", ui), slot=slot_of[ui]))
-            ops.append(op)
-        gp.nslots = max(1, len(self._param_units))
+        fwd_ops, ops, gp.nslots, w = self.sweep_ops(p)
+        gp.fwd = self._build(nbits, fwd_ops, adjoint=False)
         half = bp << self.n
         # with several instances the tile's non-pair bits must stay below the
         # instance bits, so the tile takes at most n of them
@@ -333,14 +325,31 @@ class BatchedAdjoint:
         gp.sums = torch.empty(2 * gp.nslots * bp, dtype=torch.float64, device=self.dev)
         gp.e = torch.empty(2 * bp, dtype=torch.float64, device=self.dev)
         gp.ws = torch.empty(16 * bp * 1024 + 256, dtype=torch.uint8, device=self.dev)
-        # gradient = W @ Im<lam|G|psi>, W[param, slot] = scale: a fixed-order (deterministic)
-        # sum over the gates that share a parameter
-        w = np.zeros((self.circuit.num_params, gp.nslots))
-        for s_, u in enumerate(self._param_units):
-            w[self._units[u].index, s_] += self._units[u].scale
         gp.weights = torch.from_numpy(w).to(self.dev)
         gp.grads = torch.zeros(self.circuit.num_params, bp, dtype=torch.float64, device=self.dev)
         return gp
+
+    def sweep_ops(self, p: np.ndarray) -> Tuple[List[Op], List[Op], int, np.ndarray]:
+        """Op lists of one gradient evaluation of the (padded) parameter rows
+        `p`: the forward ops, the backward sweep (inverse gates in reverse
+        order, each parameterised unit preceded by its EXPECT op), the number
+        of EXPECT slots and the weights W (parameters x slots): gradient =
+        W Im<lam|G|psi>, W[param, slot] = the unit's scale, so that gates
+        sharing a parameter are summed in a fixed (deterministic) order."""
+        fwd = [op for _, op in self._gate_ops(p, False)]
+        inv = self._gate_ops(p, True)
+        slot_of = {u: s for s, u in enumerate(self._param_units)}
+        ops: List[Op] = []
+        for ui, op in reversed(inv):
+            un = self._units[ui]
+            if un.fixed is None:
+                ops.append(Op("expect", op.tbits, (), un.gen, tag=("expect", ui), slot=slot_of[ui]))
+            ops.append(op)
+        nslots = max(1, len(self._param_units))
+        w = np.zeros((self.circuit.num_params, nslots))
+        for s_, u in enumerate(self._param_units):
+            w[self._units[u].index, s_] += self._units[u].scale
+        return fwd, ops, nslots, w
 
     def _build(self, nbits: int, ops: Sequence[Op], adjoint: bool, k: Optional[int] = None,
                pair: Optional[int] = None):

@@ -55,17 +55,47 @@ def tune_qaoa_size(tuner: Autotuner, n: int, precision: str, device_id: int = 0,
 
 
 class UnevenQAOABatch:
-    """`jit_min_qubits`: instances of at least that many qubits run their
-    register passes as run-time compiled kernels (their kernels dominate the
-    replay); smaller ones keep the generic kernels, whose per-instance
-    compilation would not pay off.  Tile widths come per qubit count from the
-    autotuner's "qaoa" entries (`autotune=True` tunes sizes it has none for,
-    on the first instance of that size)."""
+    """Two ways to run the batch:
+
+    mode="persistent": every instance's whole gradient (forward passes,
+      lam = C psi and the energy, adjoint sweep, final sums) is planned into
+      the work list of ONE persistent kernel launch (``PersistentBatch``);
+      a replay is a control-word memset plus that launch.  `caps` (forward,
+      pair tile-width caps) come from the autotuner's "batch" entry for this
+      workload, else the defaults; ``tune_caps`` measures them.
+    mode="graph": each instance runs its own kernel chain; the chains are
+      captured over several streams into one CUDA graph.  `jit_min_qubits`:
+      instances of at least that many qubits run their register passes as
+      run-time compiled kernels (their kernels dominate the replay); smaller
+      ones keep the generic kernels, whose per-instance compilation would not
+      pay off.  Tile widths come per qubit count from the autotuner's "qaoa"
+      entries (`autotune=True` tunes sizes it has none for, on the first
+      instance of that size)."""
 
     def __init__(self, instances, precision: str = "single", device_id: int = 0, streams: int = 16,
-                 jit_min_qubits: int = 22, autotune: bool = False, tuner: Optional[Autotuner] = None):
+                 jit_min_qubits: int = 22, autotune: bool = False, tuner: Optional[Autotuner] = None,
+                 mode: str = "graph", caps: Optional[Tuple[int, int]] = None, label: Optional[str] = None):
+        if mode not in ("graph", "persistent"):
+            raise ValueError(f"mode must be 'graph' or 'persistent', not {mode!r}")
         self.instances = instances
+        self.mode = mode
         self.jit_min_qubits = jit_min_qubits
+        self.captured_launches = 0
+        self.graph = None
+        if mode == "persistent":
+            from .persistent import PersistentBatch, batch_key
+            tuner = tuner or Autotuner()
+            dev = torch.device("cuda", device_id)
+            self.caps = caps
+            if self.caps is None and label is not None:
+                self.caps = tuner.lookup_adjoint(batch_key(torch.cuda.get_device_name(dev), precision, label))
+            self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision,
+                                           device_id) for n, edges, p, _ in instances]
+            self.persistent = PersistentBatch([(e, np.asarray(prm)) for e, (_, _, _, prm) in
+                                               zip(self.engines, instances)], precision, device_id, caps=self.caps)
+            self.caps = self.persistent.caps
+            self.dev = self.persistent.dev
+            return
         tuner = tuner or Autotuner()
         dev = torch.device("cuda", device_id)
         esize = 8 if precision == "single" else 16
@@ -91,6 +121,24 @@ class UnevenQAOABatch:
         self.nstreams = streams
         self.graph = None
 
+    def tune_caps(self, label: str, tuner: Optional[Autotuner] = None):
+        """Persistent mode: time every tile-width cap candidate on this batch,
+        store the fastest under the "batch" key of `label` and rebuild the
+        batch with it; returns (caps, ms, trials)."""
+        from .persistent import PersistentBatch, batch_key, tune
+        if self.mode != "persistent":
+            raise ValueError("tune_caps applies to mode='persistent'")
+        prec = self.persistent.precision
+        probs = [(e, np.asarray(prm)) for e, (_, _, _, prm) in zip(self.engines, self.instances)]
+        key = batch_key(torch.cuda.get_device_name(self.dev), prec, label)
+        self.persistent = None
+        best, ms, trials = tune(lambda caps: PersistentBatch(probs, prec, self.dev.index, caps=caps), prec, key,
+                                tuner)
+        self.persistent = PersistentBatch(probs, prec, self.dev.index, caps=best)
+        self.caps = best
+        self.graph = None
+        return best, ms, trials
+
     @property
     def num_gradients(self) -> int:
         return sum(2 * p for _, _, p, _ in self.instances)
@@ -115,8 +163,13 @@ class UnevenQAOABatch:
     def capture(self):
         """Warm up (first-launch configuration and the compilation of the
         generated pass kernels happen outside capture), then capture every
-        instance's chain into one CUDA graph."""
+        instance's chain (mode "graph") or the persistent launch into one
+        CUDA graph."""
         from .. import _native as N
+        if self.mode == "persistent":
+            self.graph = self.persistent.capture()
+            self.captured_launches = 1  # the kernel (plus a memset node of the control words)
+            return self.graph
         self.run_eager()
         N.jit_wait(900)
         self.run_eager()  # loads the compiled kernels on this device
@@ -136,6 +189,8 @@ class UnevenQAOABatch:
 
     def results(self) -> List[Tuple[float, np.ndarray]]:
         """[(energy, gradient (2p,))] per instance (host copies)."""
+        if self.mode == "persistent":
+            return self.persistent.results()
         out = []
         for gp in self.plans:
             out.append((float(gp.energies[0]), gp.gradients[0].cpu().numpy()))
