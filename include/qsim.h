@@ -294,12 +294,19 @@ typedef struct qs_batch_sizes {
   int32_t nstages;          /* register stages over all instances                */
   int32_t big;              /* some pass needs the wide dense-op code paths      */
   int32_t dtype;
-  int32_t pad;
+  int32_t jit_fns;          /* generated register-stage functions (see below)   */
+  uint64_t jit_key;         /* identifies them for qs_batch_launch               */
 } qs_batch_sizes;
 
 /* Plan a batch on the host.  Every stage of every problem (register passes,
  * lam = H psi with the energy partials, the final reduction) is cut into
  * work items of `tiles_per_item` tiles / `amps_per_ham_item` amplitudes.
+ * mats_host (the matrix table in HOST memory, the state's precision; may be
+ * NULL): the register stages of problems with at least jit_min_qubits
+ * qubits are also generated as straight-line device functions (as
+ * qs_apply_fused_ex generates kernels), queued for compilation (NVRTC,
+ * relocatable) when the plan is written, and linked with the batch kernel
+ * (nvJitLink) at the first qs_batch_launch that finds them compiled.
  * blob == NULL: only fill *sizes (and state_off[i], the element offset of
  * problem i's pair vector in the state pool, if state_off != NULL); else
  * write the plan (blob_bytes >= sizes->blob_bytes).  Passes follow the rules
@@ -308,10 +315,18 @@ typedef struct qs_batch_sizes {
  * passes share one k.  No reference counterpart (the reference has neither
  * gradients nor batching). */
 int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, const qs_pass* passes, int npasses,
-                  const qs_op* ops, int64_t nops, int64_t mats_count, const uint64_t* xmask,
+                  const qs_op* ops, int64_t nops, int64_t mats_count, const void* mats_host,
+                  int jit_min_qubits, const uint64_t* xmask,
                   const uint64_t* zmask, const double* coeff, int nterms_total, const double* weights,
                   int64_t nweights, int64_t tiles_per_item, int64_t amps_per_ham_item, void* blob,
                   size_t blob_bytes, qs_batch_sizes* sizes, int64_t* state_off);
+
+/* Compile and link the generated functions of a plan with the batch kernel
+ * (waiting for their compilation) without loading the result: no device is
+ * needed.  *cubin_bytes <- the linked cubin's size (0 for a plan without
+ * generated functions).  QS_ENOTSUP with the compiler's or linker's message
+ * when a step fails. */
+int qs_batch_link_check(const qs_batch_sizes* sizes, int64_t* cubin_bytes);
 
 /* Run a planned batch as ONE persistent kernel launch (after a memset of the
  * control words, both on `stream`).  blob_dev: the plan in device memory
@@ -321,7 +336,11 @@ int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, const qs_pass
  * device memory.  Work items wait for their problem's earlier stages with a
  * bounded wait of timeout_s seconds; a wait that gives up stores
  * (1 << 32) | item in control word 1 (bytes 8..15 of ctrl, 0 on success) and
- * the launch ends early.  Replaces nothing in the reference (see above). */
+ * the launch ends early.  A plan with generated functions runs as the
+ * linked kernel once it is linked on this device (returns 1), else as the
+ * generic kernel (returns QS_OK), with the same results up to rounding;
+ * during stream capture nothing is compiled or linked, so warm up first.
+ * Replaces nothing in the reference (see above). */
 int qs_batch_launch(const qs_batch_sizes* sizes, const void* blob_dev, void* states, const void* mats,
                     double* partials, double* energies, double* grads, void* ctrl, size_t ctrl_bytes,
                     double timeout_s, void* stream);

@@ -104,12 +104,13 @@ class qs_batch_sizes(C.Structure):
         ("nstages", C.c_int32),
         ("big", C.c_int32),
         ("dtype", C.c_int32),
-        ("pad", C.c_int32),
+        ("jit_fns", C.c_int32),
+        ("jit_key", C.c_uint64),
     ]
 
 
 assert C.sizeof(qs_op) == 80
-assert C.sizeof(qs_batch_inst) == 48 and C.sizeof(qs_batch_sizes) == 80
+assert C.sizeof(qs_batch_inst) == 48 and C.sizeof(qs_batch_sizes) == 88
 assert C.sizeof(qs_pass) == 8 + 4 * QS_MAX_TILE_BITS + 16
 
 _vp, _i, _i64, _u64, _d, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
@@ -147,8 +148,9 @@ SIGNATURES = {
     "qs_adjoint_pair_ex": (_i, [_vp, _i, _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _vp, _vp, _i64, _vp,
                                 _i64, _vp]),
     "qs_batch_plan": (_i, [_i, C.POINTER(qs_batch_inst), _i, C.POINTER(qs_pass), _i, C.POINTER(qs_op), _i64, _i64,
-                           _vp, _vp, _vp, _i, _vp, _i64, _i64, _i64, _vp, _sz, C.POINTER(qs_batch_sizes),
+                           _vp, _i, _vp, _vp, _vp, _i, _vp, _i64, _i64, _i64, _vp, _sz, C.POINTER(qs_batch_sizes),
                            C.POINTER(C.c_int64)]),
+    "qs_batch_link_check": (_i, [C.POINTER(qs_batch_sizes), C.POINTER(C.c_int64)]),
     "qs_batch_launch": (_i, [C.POINTER(qs_batch_sizes), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _d, _vp]),
     "qs_jit_shutdown": (_i, []),
     "qs_jit_set_mode": (_i, [_i]),

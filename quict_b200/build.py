@@ -45,6 +45,30 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+# the persistent batch kernel as relocatable device code (linked at run time
+# with generated register-stage functions), embedded in the library
+RDC_SRC = os.path.join(CSRC, "rdc", "batch_dev.cu")
+RDC_CUBIN = os.path.join(OBJDIR, "batch_dev.cubin")
+RDC_C = os.path.join(OBJDIR, "batch_dev_cubin.c")
+RDC_OBJ = os.path.join(OBJDIR, "batch_dev_cubin.o")
+
+
+def embed_cubin(cubin: str, csrc: str, obj: str) -> None:
+    """Write the cubin as a C byte array (qs_batch_dev_cubin) and compile it."""
+    data = open(cubin, "rb").read()
+    with open(csrc, "w") as f:
+        f.write("/* generated by quict_b200/build.py from csrc/rdc/batch_dev.cu */\n")
+        f.write(f"const unsigned long long qs_batch_dev_cubin_size = {len(data)}ull;\n")
+        f.write("__attribute__((aligned(16))) const unsigned char qs_batch_dev_cubin[] = {\n")
+        for i in range(0, len(data), 32):
+            f.write(",".join(str(b) for b in data[i:i + 32]) + ",\n")
+        f.write("};\n")
+    r = subprocess.run(["gcc", "-O0", "-fPIC", "-c", csrc, "-o", obj], capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("compile of the embedded batch cubin failed")
+
+
 def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
     srcs = sources()
@@ -59,6 +83,13 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False)
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)
+    rdc_stale = force or ptxas_verbose or _stale(RDC_CUBIN, [RDC_SRC] + hdrs)
+    if rdc_stale:
+        cmd = [nvcc(), "-arch=sm_100a", "-rdc=true", "-cubin", "-O3", "-lineinfo", "-std=c++17",
+               "--expt-relaxed-constexpr", "-I", INCLUDE, RDC_SRC, "-o", RDC_CUBIN]
+        if ptxas_verbose:
+            cmd += ["-Xptxas", "-v"]
+        jobs.append(cmd)
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -71,6 +102,9 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False)
                 raise RuntimeError(f"nvcc failed: {' '.join(cmd)}")
             if ptxas_verbose or (r.stderr.strip() and not quiet):
                 sys.stderr.write(r.stderr)
+    if rdc_stale or _stale(RDC_OBJ, [RDC_CUBIN]):
+        embed_cubin(RDC_CUBIN, RDC_C, RDC_OBJ)
+    objs.append(RDC_OBJ)
     if force or jobs or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -27,245 +27,26 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
+#include "batch.cuh"
 #include "common.cuh"
+#include "jit.h"
 #include "regtile.cuh"
 
 namespace qs {
 namespace {
-
-enum : int32_t { BI_FWD = 0, BI_HAM = 1, BI_BWD = 2, BI_FIN = 3 };
-
-struct __align__(16) BItem {
-    int32_t kind;     // BI_*
-    int32_t inst;     // instance
-    int32_t stage;    // FWD / BWD: index of the stage's BArgs; HAM: index of the item within the HAM stage
-    int32_t fresh;    // FWD: the pass reads |0...0> instead of psi
-    int64_t need;     // items of this instance that finish before this one starts
-    uint64_t t0, t1;  // FWD / BWD: tile range; HAM: amplitude range of psi
-};
-
-struct __align__(16) BInst {
-    int32_t n, nslots, nparams, nham;
-    int32_t term_begin, nterms, tiles_bwd, pad;
-    int64_t state_off;  // elements: the pair vector (psi: 2^n amplitudes, then lam)
-    int64_t part_off;   // doubles: EXPECT partials (2 nslots tiles_bwd), then HAM partials (2 nham)
-    int64_t w_off;      // doubles of the blob's weight array: W (nparams x nslots, row-major)
-    int64_t grad_off;   // doubles of the gradient output
-};
-
-struct __align__(16) BTerm {  // an instance's terms are sorted (stably) by x
-    uint64_t x, z;
-    double cre, cim;  // coefficient times i^popc(x & z)
-};
-
-struct __align__(16) BArgs {  // a planned register pass; its arrays sit elsewhere in the blob
-    RegHead h;
-    int64_t off_st, off_ops, off_cp, off_es;  // byte offsets in the blob
-};
-
-struct __align__(16) BHead {
-    int32_t ninst, nitems, nstages, dtype;
-    int32_t threads, big, pad0, pad1;
-    int64_t off_items, off_inst, off_args, off_terms, off_w;
-    int64_t smem;
-};
-
-// control words (ctrl): [0] next item, [1] error (0, or (1 << 32) | item whose
-// wait timed out), [2], [3] unused, [4 + i] items of instance i done
-constexpr int kCtrlHead = 4;
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Block sum of (a, b) in a fixed order; the result is valid in thread 0.
-__device__ __forceinline__ double2 block_sum(double a, double b) {
-    __shared__ double2 red[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        b += __shfl_xor_sync(0xffffffffu, b, o);
-    }
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_double2(a, b);
-    __syncthreads();
-    double2 s = make_double2(0.0, 0.0);
-    if (threadIdx.x == 0)
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-            s.x += red[w].x;
-            s.y += red[w].y;
-        }
-    return s;
-}
-
-// lam[j] = sum_t c_t (-1)^popc(z_t & (j ^ x_t)) psi[j ^ x_t] for j in [j0, j1),
-// and the FP64 partial of <psi|lam> over the range (lam as stored).  psi was
-// written by other CTAs of this launch: it is read through L2 (ld.cg).
-template <typename V>
-__device__ void ham_range(V* __restrict__ pl, const BInst& I, const BTerm* __restrict__ tm, uint64_t j0, uint64_t j1,
-                          double* __restrict__ out) {
-    const uint64_t N = uint64_t(1) << I.n;
-    const V* psi = pl;
-    V* lam = pl + N;
-    double er = 0.0, ei = 0.0;
-    for (uint64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        double re = 0.0, im = 0.0;
-        int t = 0;
-        while (t < I.nterms) {
-            const uint64_t x = tm[t].x;
-            const uint64_t src = j ^ x;
-            const V a = __ldcg(psi + src);
-            double sr = 0.0, si = 0.0;
-            for (; t < I.nterms && tm[t].x == x; ++t) {
-                const bool neg = __popcll(tm[t].z & src) & 1;
-                sr += neg ? -tm[t].cre : tm[t].cre;
-                si += neg ? -tm[t].cim : tm[t].cim;
-            }
-            const double ar = double(a.x), ai = double(a.y);
-            re += sr * ar - si * ai;
-            im += sr * ai + si * ar;
-        }
-        const V lv = mk<V>(re, im);
-        lam[j] = lv;
-        const V u = __ldcg(psi + j);
-        er += double(u.x) * double(lv.x) + double(u.y) * double(lv.y);
-        ei += double(u.x) * double(lv.y) - double(u.y) * double(lv.x);
-    }
-    const double2 s = block_sum(er, ei);
-    if (threadIdx.x == 0) {
-        out[0] = s.x;
-        out[1] = s.y;
-    }
-}
-
-// energy (re, im) = sum of the HAM partials; gradient[k] = sum_s W[k, s] *
-// Im(sum over tiles of slot s's EXPECT partials).  `scratch`: nslots doubles
-// of shared memory.
-__device__ void finish(const BInst& I, const double* __restrict__ parts, const double* __restrict__ W,
-                       double* __restrict__ energy, double* __restrict__ grads, double* __restrict__ scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const double* ep = parts + I.part_off + 2 * int64_t(I.nslots) * I.tiles_bwd;
-    if (warp == 0) {
-        double r = 0.0, i = 0.0;
-        for (int t = lane; t < I.nham; t += 32) {
-            r += __ldcg(ep + 2 * t);
-            i += __ldcg(ep + 2 * t + 1);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            r += __shfl_xor_sync(0xffffffffu, r, o);
-            i += __shfl_xor_sync(0xffffffffu, i, o);
-        }
-        if (lane == 0) {
-            energy[0] = r;
-            energy[1] = i;
-        }
-    }
-    for (int s = warp; s < I.nslots; s += nw) {
-        const double* sp = parts + I.part_off + 2 * int64_t(s) * I.tiles_bwd;
-        double im = 0.0;
-        for (int t = lane; t < I.tiles_bwd; t += 32) im += __ldcg(sp + 2 * t + 1);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) im += __shfl_xor_sync(0xffffffffu, im, o);
-        if (lane == 0) scratch[s] = im;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < I.nparams; k += blockDim.x) {
-        const double* w = W + I.w_off + int64_t(k) * I.nslots;
-        double g = 0.0;
-        for (int s = 0; s < I.nslots; ++s) g += w[s] * scratch[s];
-        grads[I.grad_off + k] = g;
-    }
-}
-
-// One register stage's tiles [t0, t1); a call (not inlined), so that each
-// body is optimised on its own.
-template <typename V, int R, bool EXP>
-__device__ __noinline__ void batch_pass(V* __restrict__ vec, const RegHead& h, const KStage* __restrict__ st,
-                                        const KOp* __restrict__ ops, const KCopy* __restrict__ cp,
-                                        const int* __restrict__ es, const V* __restrict__ mats,
-                                        double* __restrict__ partials, uint64_t t0, uint64_t t1, bool fresh) {
-    reg_tiles<V, R, EXP, false>(vec, h, st, ops, cp, es, mats, partials, t0, t1, 1, fresh);
-}
 
 template <typename V, int R>
 __global__ void __launch_bounds__(256, 1)
 k_batch(const unsigned char* __restrict__ blob, V* __restrict__ states, const V* __restrict__ mats,
         double* __restrict__ parts, double* __restrict__ energies, double* __restrict__ grads,
         unsigned long long* __restrict__ ctrl, uint64_t timeout_ns) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const BHead& hd = *reinterpret_cast<const BHead*>(blob);
-    const BItem* items = reinterpret_cast<const BItem*>(blob + hd.off_items);
-    const BInst* insts = reinterpret_cast<const BInst*>(blob + hd.off_inst);
-    const BArgs* args = reinterpret_cast<const BArgs*>(blob + hd.off_args);
-    const BTerm* terms = reinterpret_cast<const BTerm*>(blob + hd.off_terms);
-    const double* W = reinterpret_cast<const double*>(blob + hd.off_w);
-    unsigned long long* next = ctrl;
-    unsigned long long* err = ctrl + 1;
-    unsigned long long* done = ctrl + kCtrlHead;
-    __shared__ long long s_item;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            long long it = (long long)atomicAdd(next, 1ull);
-            if (it < hd.nitems) {
-                const BItem& I = items[it];
-                const unsigned long long need = (unsigned long long)I.need;
-                if (need > 0 && ld_acquire(done + I.inst) < need) {
-                    const uint64_t start = global_ns();
-                    while (ld_acquire(done + I.inst) < need) {
-                        if (*reinterpret_cast<volatile unsigned long long*>(err) != 0ull) {
-                            it = -1;
-                            break;
-                        }
-                        if (global_ns() - start > timeout_ns) {
-                            atomicCAS(err, 0ull, (1ull << 32) | (unsigned long long)it);
-                            it = -1;
-                            break;
-                        }
-                        __nanosleep(256);
-                    }
-                }
-                __threadfence();
-            }
-            s_item = it;
-        }
-        __syncthreads();
-        const long long it = s_item;
-        if (it < 0 || it >= hd.nitems) return;
-        const BItem& I = items[it];
-        const BInst& S = insts[I.inst];
-        V* pl = states + S.state_off;
-        if (I.kind == BI_FWD || I.kind == BI_BWD) {
-            const BArgs& A = args[I.stage];
-            const KStage* st = reinterpret_cast<const KStage*>(blob + A.off_st);
-            const KOp* ops = reinterpret_cast<const KOp*>(blob + A.off_ops);
-            const KCopy* cp = reinterpret_cast<const KCopy*>(blob + A.off_cp);
-            const int* es = reinterpret_cast<const int*>(blob + A.off_es);
-            if (I.kind == BI_FWD)
-                batch_pass<V, R, false>(pl, A.h, st, ops, cp, es, mats, nullptr, I.t0, I.t1, I.fresh != 0);
-            else
-                batch_pass<V, R, true>(pl, A.h, st, ops, cp, es, mats, parts + S.part_off, I.t0, I.t1, false);
-        } else if (I.kind == BI_HAM) {
-            ham_range<V>(pl, S, terms + S.term_begin, I.t0, I.t1,
-                         parts + S.part_off + 2 * int64_t(S.nslots) * S.tiles_bwd + 2 * int64_t(I.stage));
-        } else {
-            finish(S, parts, W, energies + 2 * int64_t(I.inst), grads, reinterpret_cast<double*>(smem_raw));
-        }
-        __syncthreads();  // the item's stores are done; shared memory is free again
-        if (threadIdx.x == 0) {
-            __threadfence();
-            atomicAdd(done + I.inst, 1ull);
-        }
-    }
+    batch_loop<V, R, false>(blob, states, mats, parts, energies, grads, ctrl, timeout_ns);
 }
 
 // ------------------------------------------------------------------ host side
@@ -290,13 +71,46 @@ struct Stage {
     int fresh;
 };
 
+uint64_t fnv64(const std::string& t, uint64_t h = 1469598103934665603ull) {
+    for (unsigned char c : t) h = (h ^ c) * 1099511628211ull;
+    return h;
+}
+
+// Generated register-stage functions of planned batches, by the plan's
+// jit_key: compile-cache keys of the functions (in dispatcher index order)
+// and the dispatcher source.
+struct BatchFns {
+    std::vector<std::string> keys;
+    std::string dispatcher;
+};
+std::mutex g_fns_mu;
+std::unordered_map<uint64_t, std::shared_ptr<BatchFns>> g_fns;
+
+std::string dispatcher_source(const std::vector<std::string>& names, bool c128) {
+    std::string d = "typedef unsigned long long u64;\ntypedef unsigned int u32;\n";
+    d += c128 ? "typedef double2 V;\n" : "typedef float2 V;\n";
+    for (const auto& n : names)
+        d += "extern \"C\" __device__ void " + n + "(V*, const void*, const V*, double*, u64, u64, u32);\n";
+    d += "extern \"C\" __device__ int qs_batch_jit(int fn, void* vec, const void* params, const void* mats, "
+         "double* partials, u64 t0, u64 t1, u32 zero_in) {\n  switch (fn) {\n";
+    for (size_t i = 0; i < names.size(); ++i)
+        d += "  case " + std::to_string(i) + ": " + names[i] +
+             "((V*)vec, params, (const V*)mats, partials, t0, t1, zero_in); return 1;\n";
+    d += "  default: return 0;\n  }\n}\n";
+    return d;
+}
+
 }  // namespace
 }  // namespace qs
 
 using namespace qs;
 
+extern "C" const unsigned long long qs_batch_dev_cubin_size;
+extern "C" const unsigned char qs_batch_dev_cubin[];
+
 extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, const qs_pass* passes, int npasses,
-                             const qs_op* ops, int64_t nops, int64_t mats_count, const uint64_t* xmask,
+                             const qs_op* ops, int64_t nops, int64_t mats_count, const void* mats_host,
+                             int jit_min_qubits, const uint64_t* xmask,
                              const uint64_t* zmask, const double* coeff, int nterms_total, const double* weights,
                              int64_t nweights, int64_t tiles_per_item, int64_t amps_per_ham_item, void* blob,
                              size_t blob_bytes, qs_batch_sizes* sizes, int64_t* state_off) {
@@ -314,6 +128,8 @@ extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, co
     std::vector<BTerm> terms;
     std::vector<double> wts;
     int big = 0, maxnt = 5;
+    std::vector<std::string> fn_names, fn_srcs;  // generated register-stage functions
+    std::unordered_map<std::string, int> fn_index;
     size_t smem = 0;
     int64_t state_elems = 0, part_doubles = 0, grad_doubles = 0;
     static thread_local RegArgs ra;
@@ -412,12 +228,42 @@ extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, co
                                                          : reg_smem_bytes<float2>(ra, R, bwd);
                     smem = std::max(smem, need);
                     maxnt = std::max(maxnt, ra.nT);
-                    // compact record: BArgs, then stages, ops, copies, EXPECT slots
+                    // a generated function for the linked kernel (large problems)
+                    int32_t jit_fn = -1;
+                    std::vector<uint64_t> params;
+                    if (mats_host != nullptr && q.n >= jit_min_qubits) {
+                        static const char kSlot[] = "qs_pf_name_slot";
+                        std::string src;
+                        size_t jsmem = 0;
+                        int jthreads = 0;
+                        if (gen_batch_pass(&ra, R, dtype == QS_C128, mats_host, kSlot, &src, &params, &jsmem,
+                                           &jthreads)) {
+                            // the function's name: a hash of its text (equal passes share one function)
+                            char nm[40];
+                            snprintf(nm, sizeof(nm), "qs_pf_%016llx%c", (unsigned long long)fnv64(src),
+                                     dtype == QS_C128 ? 'd' : 's');
+                            for (size_t at = src.find(kSlot); at != std::string::npos; at = src.find(kSlot, at))
+                                src.replace(at, sizeof(kSlot) - 1, nm);
+                            auto f = fn_index.find(nm);
+                            if (f == fn_index.end()) {
+                                f = fn_index.emplace(nm, int(fn_names.size())).first;
+                                fn_names.push_back(nm);
+                                fn_srcs.push_back(std::move(src));
+                            }
+                            jit_fn = f->second;
+                            smem = std::max(smem, jsmem);
+                            maxnt = std::max(maxnt, 31 - __builtin_clz(unsigned(jthreads)));
+                        } else {
+                            params.clear();
+                        }
+                    }
+                    // compact record: BArgs, then stages, ops, copies, EXPECT slots, parameter block
                     const size_t o_st = align16(sizeof(BArgs));
                     const size_t o_ops = align16(o_st + sizeof(KStage) * size_t(ra.nstages));
                     const size_t o_cp = align16(o_ops + sizeof(KOp) * size_t(ra.nops));
                     const size_t o_es = align16(o_cp + sizeof(KCopy) * size_t(ra.nops));
-                    const size_t tot = align16(o_es + sizeof(int) * size_t(ra.nexp > 0 ? ra.nexp : 1));
+                    const size_t o_pb = align16(o_es + sizeof(int) * size_t(ra.nexp > 0 ? ra.nexp : 1));
+                    const size_t tot = align16(o_pb + sizeof(uint64_t) * params.size());
                     std::vector<unsigned char> rec(tot, 0);
                     BArgs ba;
                     memset(&ba, 0, sizeof(ba));
@@ -426,6 +272,9 @@ extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, co
                     ba.off_ops = int64_t(o_ops);
                     ba.off_cp = int64_t(o_cp);
                     ba.off_es = int64_t(o_es);
+                    ba.jit_fn = jit_fn;
+                    ba.off_params = int64_t(o_pb);
+                    if (!params.empty()) memcpy(rec.data() + o_pb, params.data(), sizeof(uint64_t) * params.size());
                     memcpy(rec.data(), &ba, sizeof(ba));
                     memcpy(rec.data() + o_st, ra.st, sizeof(KStage) * size_t(ra.nstages));
                     memcpy(rec.data() + o_ops, ra.ops, sizeof(KOp) * size_t(ra.nops));
@@ -527,6 +376,12 @@ extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, co
     sizes->nstages = int32_t(arg_blobs.size());
     sizes->big = big;
     sizes->dtype = dtype;
+    sizes->jit_fns = int32_t(fn_names.size());
+    {
+        uint64_t key = fnv64(dtype == QS_C128 ? "c128" : "c64");
+        for (const auto& nm : fn_names) key = fnv64(nm, key);
+        sizes->jit_key = fn_names.empty() ? 0 : key;
+    }
     if (state_off != nullptr)
         for (int i = 0; i < ninst; ++i) state_off[i] = bi[size_t(i)].state_off;
     if (blob == nullptr) return QS_OK;  // size query
@@ -560,15 +415,51 @@ extern "C" int qs_batch_plan(int dtype, const qs_batch_inst* inst, int ninst, co
         ba.off_ops += int64_t(rec_at[k]);
         ba.off_cp += int64_t(rec_at[k]);
         ba.off_es += int64_t(rec_at[k]);
+        ba.off_params += int64_t(rec_at[k]);
         memcpy(out + o_args + sizeof(BArgs) * k, &ba, sizeof(ba));
         memcpy(out + rec_at[k], arg_blobs[k].data(), arg_blobs[k].size());
     }
     if (!terms.empty()) memcpy(out + o_terms, terms.data(), sizeof(BTerm) * terms.size());
     if (!wts.empty()) memcpy(out + o_w, wts.data(), sizeof(double) * wts.size());
+    if (!fn_names.empty()) {  // queue the functions' compilation (host threads) and record the batch
+        auto b = std::make_shared<BatchFns>();
+        for (size_t k = 0; k < fn_names.size(); ++k) {
+            b->keys.push_back(jit::queue_device_fn(fn_srcs[k], fn_names[k].c_str()));
+            if (b->keys.back().empty()) {
+                set_error("qs_batch_plan: run-time compilation is unavailable: %s", jit::last_log());
+                return QS_ENOTSUP;
+            }
+        }
+        b->dispatcher = dispatcher_source(fn_names, dtype == QS_C128);
+        std::lock_guard<std::mutex> lock(g_fns_mu);
+        g_fns[sizes->jit_key] = b;
+    }
     return QS_OK;
 }
 
 namespace {
+// The linked kernel of a plan with generated functions, when it can run now
+// (null: run the generic kernel).  Outside stream capture the first launch
+// links and loads it (after the compilations in mode QS_JIT_SYNC; in mode
+// QS_JIT_ASYNC only once they are done).
+void* linked_kernel(const qs_batch_sizes& sz, cudaStream_t st, int* occ) {
+    if (sz.jit_fns <= 0 || jit::mode() == QS_JIT_OFF) return nullptr;
+    std::shared_ptr<BatchFns> b;
+    {
+        std::lock_guard<std::mutex> lock(g_fns_mu);
+        auto it = g_fns.find(sz.jit_key);
+        if (it == g_fns.end()) return nullptr;
+        b = it->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    return jit::link_module(sz.jit_key, qs_batch_dev_cubin, size_t(qs_batch_dev_cubin_size), b->dispatcher, b->keys,
+                            sz.dtype == QS_C128 ? "qs_batch_linked_c128" : "qs_batch_linked_c64",
+                            jit::mode() == QS_JIT_SYNC && !capturing, !capturing, sz.threads, size_t(sz.smem_bytes),
+                            occ);
+}
+
 template <typename V, int R>
 int launch_batch(const qs_batch_sizes& sz, const void* blob, void* states, const void* mats, double* parts,
                  double* energies, double* grads, void* ctrl, uint64_t timeout_ns, cudaStream_t st) {
@@ -581,12 +472,23 @@ int launch_batch(const qs_batch_sizes& sz, const void* blob, void* states, const
                   (long long)sz.smem_bytes);
         return QS_ENOTSUP;
     }
+    int locc = 0;
+    void* lfn = linked_kernel(sz, st, &locc);
+    if (lfn != nullptr) occ = locc;
     int64_t grid = int64_t(sm_count()) * occ;
     if (grid > sz.nitems) grid = sz.nitems;
     cudaError_t e = cudaMemsetAsync(ctrl, 0, size_t(sz.ctrl_bytes), st);
     if (e != cudaSuccess) {
         set_error("qs_batch_launch: cudaMemsetAsync: %s", cudaGetErrorString(e));
         return QS_ECUDA;
+    }
+    if (lfn != nullptr) {
+        const unsigned char* b = static_cast<const unsigned char*>(blob);
+        const void* m = mats;
+        void* c = ctrl;
+        void* params[] = {&b, &states, &m, &parts, &energies, &grads, &c, &timeout_ns};
+        const int rc = jit::launch(lfn, unsigned(grid), unsigned(sz.threads), size_t(sz.smem_bytes), st, params);
+        return rc ? rc : 1;
     }
     fn<<<unsigned(grid), unsigned(sz.threads), size_t(sz.smem_bytes), st>>>(
         static_cast<const unsigned char*>(blob), static_cast<V*>(states), static_cast<const V*>(mats), parts, energies,
@@ -595,6 +497,27 @@ int launch_batch(const qs_batch_sizes& sz, const void* blob, void* states, const
     return QS_OK;
 }
 }  // namespace
+
+extern "C" int qs_batch_link_check(const qs_batch_sizes* sizes, int64_t* cubin_bytes) {
+    QS_REQUIRE(sizes != nullptr && cubin_bytes != nullptr, "null argument");
+    *cubin_bytes = 0;
+    if (sizes->jit_fns <= 0) return QS_OK;
+    std::shared_ptr<BatchFns> b;
+    {
+        std::lock_guard<std::mutex> lock(g_fns_mu);
+        auto it = g_fns.find(sizes->jit_key);
+        QS_REQUIRE(it != g_fns.end(), "qs_batch_link_check: the plan's functions are not registered");
+        b = it->second;
+    }
+    const std::string cubin =
+        jit::link_cubin(qs_batch_dev_cubin, size_t(qs_batch_dev_cubin_size), b->dispatcher, b->keys, true);
+    if (cubin.empty()) {
+        set_error("qs_batch_link_check: %s", jit::last_log());
+        return QS_ENOTSUP;
+    }
+    *cubin_bytes = int64_t(cubin.size());
+    return QS_OK;
+}
 
 extern "C" int qs_batch_launch(const qs_batch_sizes* sizes, const void* blob_dev, void* states, const void* mats,
                                double* partials, double* energies, double* grads, void* ctrl, size_t ctrl_bytes,

@@ -285,15 +285,15 @@ template <typename V, int R, bool EXP, bool BIG>
 __global__ void __launch_bounds__(256, 1) k_fused_reg(V* __restrict__ vec, const __grid_constant__ RegArgs p,
                                                       const V* __restrict__ mats, double* __restrict__ partials) {
     const uint64_t ntiles = uint64_t(1) << (p.n - p.K);
+    uint64_t tile = blockIdx.x, tend = ntiles, tstep = gridDim.x;
     if (p.batched) {
         const uint64_t chunk = (ntiles + gridDim.x - 1) / gridDim.x;
-        const uint64_t tile = uint64_t(blockIdx.x) * chunk;
-        reg_tiles<V, R, EXP, BIG>(vec, p, p.st, p.ops, p.cp, p.eslot, mats, partials, tile,
-                                  tile + chunk < ntiles ? tile + chunk : ntiles, 1, false);
-    } else {
-        reg_tiles<V, R, EXP, BIG>(vec, p, p.st, p.ops, p.cp, p.eslot, mats, partials, blockIdx.x, ntiles, gridDim.x,
-                                  false);
+        tile = uint64_t(blockIdx.x) * chunk;
+        tend = tile + chunk < ntiles ? tile + chunk : ntiles;
+        tstep = 1;
     }
+    // one call: the body is inlined once
+    reg_tiles<V, R, EXP, BIG>(vec, p, p.st, p.ops, p.cp, p.eslot, mats, partials, tile, tend, tstep, false);
 }
 
 template <typename V, bool ADJ>
@@ -364,8 +364,16 @@ std::string thread_xor_expr(const uint32_t* img, int nT) {
     return e.empty() ? std::string("0u") : e;
 }
 
+// devfn != nullptr: emit the pass as `extern "C" __device__ void <devfn>(vec,
+// params, mats, partials, tile, tend, zero_in)` for the persistent batch
+// kernel instead of a kernel: it runs tiles [tile, tend) of the calling CTA,
+// reads its parameter block from global memory (params), may run in a CTA
+// wider than its own thread count (the other threads share the loads, repeat
+// the register work of thread tid mod threads, and store nothing), and with
+// zero_in != 0 reads |0...0> instead of the vector.
 template <typename V>
-bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_source = true) {
+bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_source = true,
+                  const char* devfn = nullptr) {
     constexpr bool C128 = sizeof(V) == 16;
     const int E = 1 << R, nT = a.nT, K = a.K, L = a.L, H = a.H;
     const int threads = 1 << nT, nwarps = threads / 32;
@@ -556,21 +564,33 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     g.add("struct __align__(16) P { V m[%d]; u64 ntiles; u64 gthr[8]; u64 gslot[%d]; u64 hibit[16]; u64 gctrl[%d]; "
           "u64 hsh[%d]; u64 mgoff[%d]; u64 mstride[%d]; u64 eslot[%d]; u64 misc[2];%s };\n", NM, E, NOPS, 4 * NOPS,
           NOPS, NOPS, NEXP, batched ? (" u32 pe[" + std::to_string(NM) + "];").c_str() : "");
-    g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
-          "const __grid_constant__ P p, const V* __restrict__ mats, double* __restrict__ partials) {\n", threads, minb);
+    // cooperative loops (no per-thread layout): all threads of the CTA
+    const std::string CT = devfn ? "threadIdx.x" : "tid";
+    const std::string CS = devfn ? "blockDim.x" : std::to_string(threads) + "u";
+    if (devfn) {
+        g.add("extern \"C\" __device__ void %s(V* __restrict__ vec, const void* __restrict__ pv, "
+              "const V* __restrict__ mats, double* __restrict__ partials, u64 tile, const u64 tend, "
+              "const u32 zero_in) {\n  const P& p = *reinterpret_cast<const P*>(pv);\n", devfn);
+    } else {
+        g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
+              "const __grid_constant__ P p, const V* __restrict__ mats, double* __restrict__ partials) {\n", threads,
+              minb);
+    }
     g.add("  extern __shared__ __align__(16) unsigned char smem_raw[];\n");
     g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", 1u << K);
     g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
     g.add("  double2* const ered = reinterpret_cast<double2*>(hoff + %du);\n", hoff_n);
     g.add("  V* const msm = reinterpret_cast<V*>(ered + %d);\n", a.nexp > 0 ? nwarps * a.nexp : 0);
     g.add("  V* const dsm = msm + %d;\n", batched ? NM : 0);
-    g.add("  const u32 tid = threadIdx.x;\n");
-    g.add("  for (u32 j = tid; j < %du; j += %du) { u64 o = 0;\n", 1u << H, threads);
+    if (devfn) g.add("  const u32 tid = threadIdx.x & %du;\n  const bool act = threadIdx.x < %du;\n",
+                     unsigned(threads - 1), unsigned(threads));
+    else g.add("  const u32 tid = threadIdx.x;\n");
+    g.add("  for (u32 j = %s; j < %du; j += %s) { u64 o = 0;\n", CT.c_str(), 1u << H, CS.c_str());
     g.add("#pragma unroll\n    for (int t = 0; t < %d; ++t) if ((j >> t) & 1u) o |= p.hibit[t];\n    hoff[j] = o; }\n", H);
     for (int o = 0; o < a.nops; ++o)
         if (doff[size_t(o)] >= 0)
-            g.add("  for (u32 q = tid; q < %du; q += %du) dsm[%d + q] = p.m[%d + q];\n", 1u << a.cp[o].m,
-                  unsigned(threads), doff[size_t(o)], int(a.ops[o].moff));
+            g.add("  for (u32 q = %s; q < %du; q += %s) dsm[%d + q] = p.m[%d + q];\n", CT.c_str(), 1u << a.cp[o].m,
+                  CS.c_str(), doff[size_t(o)], int(a.ops[o].moff));
     g.add("  u64 gthr = 0;\n");
     for (int i = 0; i < nT; ++i) g.add("  if ((tid >> %d) & 1u) gthr |= p.gthr[%d];\n", i, i);
     for (int si = 0; si < a.nstages; ++si) {
@@ -589,7 +609,10 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     g.add("  auto tile_base = [&](u64 t) -> u64 { u64 b = t << %d;\n", L);
     g.add("#pragma unroll\n    for (int i = 0; i < %d; ++i) { const u64 lo = p.hibit[i] - 1ull; "
           "b = ((b & ~lo) << 1) | (b & lo); }\n    return b; };\n", H);
-    if (batched) {
+    if (devfn) {  // the caller's tile range
+        g.add("  const u64 tstep = 1;\n");
+        if (batched) g.add("  u64 staged = ~0ull;\n");
+    } else if (batched) {
         // per-instance tables: contiguous runs of tiles per CTA, so that a CTA
         // restages its instance's matrices once per instance
         g.add("  const u64 chunk = (ntiles + gridDim.x - 1) / gridDim.x;\n");
@@ -601,7 +624,11 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     g.add("  __syncthreads();\n");
     const int EPC = 16 / int(sizeof(V));
     g.add("  auto prefetch = [&](V* dst, u64 base) {\n");
-    g.add("    for (u32 c = tid; c < %du; c += %du) { const u32 e = c * %du;\n", (1u << K) / EPC, threads, EPC);
+    if (devfn)
+        g.add("    if (zero_in) { for (u32 e = threadIdx.x; e < %du; e += blockDim.x) { V z; z.x = (base == 0 && e == 0) "
+              "? 1 : 0; z.y = 0; dst[e] = z; } } else\n", 1u << K);
+    g.add("    for (u32 c = %s; c < %du; c += %s) { const u32 e = c * %du;\n", CT.c_str(), (1u << K) / EPC, CS.c_str(),
+          EPC);
     g.add("      const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst + e));\n");
     g.add("      asm volatile(\"cp.async.cg.shared.global [%%0], [%%1], 16;\\n\" :: \"r\"(sa), "
           "\"l\"(vec + (base | hoff[e >> %d] | (e & %du))) : \"memory\"); }\n", L, (1u << L) - 1u);
@@ -614,7 +641,8 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     if (batched) {
         g.add("    { const u64 inst = (base & p.misc[0]) >> p.misc[1];\n");
         g.add("      if (inst != staged) {\n");
-        g.add("        for (u32 q = tid; q < %du; q += %du) { const u32 v = p.pe[q];\n", unsigned(a.nmats), threads);
+        g.add("        for (u32 q = %s; q < %du; q += %s) { const u32 v = p.pe[q];\n", CT.c_str(), unsigned(a.nmats),
+              CS.c_str());
         g.add("          if (v >> 31) { const u32 o = (v >> 16) & 0x7fffu; "
               "msm[q] = mats[p.mgoff[o] + inst * p.mstride[o] + (v & 0xffffu)]; } }\n");
         g.add("        staged = inst;\n        __syncthreads();\n      } }\n");
@@ -800,12 +828,14 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
             }
         }
     }
+    if (devfn) g.add("    if (act) {\n");
     for (int s = 0; s < E; ++s) g.add("    vec[base | gthr | p.gslot[%d]] = v%d;\n", s, var[s]);
+    if (devfn) g.add("    }\n");
     if (a.nexp > 0) {
         // per-tile partials: the warps' sums in a fixed order
         g.add("    __syncthreads();\n");
-        g.add("    for (u32 e = tid; e < %du; e += %du) { double2 t = make_double2(0.0, 0.0);\n", unsigned(a.nexp),
-              threads);
+        g.add("    for (u32 e = %s; e < %du; e += %s) { double2 t = make_double2(0.0, 0.0);\n", CT.c_str(),
+              unsigned(a.nexp), CS.c_str());
         g.add("      for (int w = 0; w < %d; ++w) { t.x += ered[w * %d + e].x; t.y += ered[w * %d + e].y; }\n", nwarps,
               NEXP, NEXP);
         g.add("      const u64 at = 2 * (p.eslot[e] * ntiles + tile);\n      partials[at] = t.x;\n"
@@ -1040,6 +1070,21 @@ int launch_pass(V* vec, int n, const qs_pass& ps, const qs_op* ops, const V* mat
 }
 
 }  // namespace
+
+bool gen_batch_pass(const void* regargs, int R, bool c128, const void* mats_host, const char* name, std::string* src,
+                    std::vector<uint64_t>* params, size_t* smem, int* threads) {
+    const RegArgs& a = *static_cast<const RegArgs*>(regargs);
+    JitPass jp;
+    const bool ok = c128 ? gen_reg_pass<double2>(a, R, static_cast<const double2*>(mats_host), jp, true, name)
+                         : gen_reg_pass<float2>(a, R, static_cast<const float2*>(mats_host), jp, true, name);
+    if (!ok) return false;
+    src->swap(jp.src);
+    params->swap(jp.params);
+    *smem = jp.smem;
+    *threads = jp.threads;
+    return true;
+}
+
 }  // namespace qs
 
 using namespace qs;

@@ -9,6 +9,8 @@
 
 #include <atomic>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -19,6 +21,7 @@
 #include <vector>
 
 #include <cuda.h>
+#include <nvJitLink.h>
 #include <nvrtc.h>
 
 #include "common.cuh"
@@ -60,9 +63,31 @@ bool sym(void* h, const char* name, F& out) {
 
 struct Entry {
     std::string src, name;
+    bool rdc = false;  // relocatable device code (a __device__ function for the linked batch kernel)
     int state = 0;  // 0 queued or compiling, 1 ready, 2 failed
     std::string cubin, log;
     double ms = 0.0;
+    void* mod[64] = {nullptr};
+    void* fn[64] = {nullptr};
+    int occ[64] = {0};
+};
+
+// nvJitLink, opened with dlopen like NVRTC (the versioned names its header
+// maps the API to).
+struct LinkApi {
+    bool tried = false, ok = false;
+    decltype(&__nvJitLinkCreate_12_9) create = nullptr;
+    decltype(&__nvJitLinkAddData_12_9) add = nullptr;
+    decltype(&__nvJitLinkComplete_12_9) complete = nullptr;
+    decltype(&__nvJitLinkGetLinkedCubinSize_12_9) cubin_size = nullptr;
+    decltype(&__nvJitLinkGetLinkedCubin_12_9) cubin = nullptr;
+    decltype(&__nvJitLinkGetErrorLogSize_12_9) log_size = nullptr;
+    decltype(&__nvJitLinkGetErrorLog_12_9) log = nullptr;
+    decltype(&__nvJitLinkDestroy_12_9) destroy = nullptr;
+};
+
+// A linked module (the batch kernel with its device functions) per device.
+struct Linked {
     void* mod[64] = {nullptr};
     void* fn[64] = {nullptr};
     int occ[64] = {0};
@@ -72,6 +97,8 @@ struct State {
     std::mutex mu;  // guards everything below and the API tables
     std::condition_variable cv;
     Api api;
+    LinkApi link;
+    std::unordered_map<uint64_t, std::shared_ptr<Linked>> linked;
     // keyed by a 128-bit hash of the source text (the text itself is kept
     // only until the entry is compiled)
     std::unordered_map<std::string, std::shared_ptr<Entry>> cache;
@@ -131,6 +158,37 @@ bool load_driver(State& s) {  // with s.mu held
     return a.cu_ok;
 }
 
+// The newest versioned name (__<base>_12_9 .. _12_0) the library exports.
+template <typename F>
+bool sym_versioned(void* h, const char* base, F& out) {
+    for (int minor = 9; minor >= 0; --minor) {
+        char nm[96];
+        snprintf(nm, sizeof(nm), "__%s_12_%d", base, minor);
+        if (sym(h, nm, out)) return true;
+    }
+    return false;
+}
+
+bool load_link(State& s) {  // with s.mu held
+    if (s.link.tried) return s.link.ok;
+    s.link.tried = true;
+    // The toolkit's copy first, by path: a framework imported earlier may have
+    // loaded an older libnvJitLink.so.12 under the same name.
+    std::string tk = std::string(getenv("CUDA_HOME") && *getenv("CUDA_HOME") ? getenv("CUDA_HOME") : "/usr/local/cuda") +
+                     "/lib64/libnvJitLink.so.12";
+    const char* names[] = {tk.c_str(), "libnvJitLink.so.12", "libnvJitLink.so", nullptr};
+    void* h = open_first(names);
+    LinkApi& a = s.link;
+    a.ok = h && sym_versioned(h, "nvJitLinkCreate", a.create) && sym_versioned(h, "nvJitLinkAddData", a.add) &&
+           sym_versioned(h, "nvJitLinkComplete", a.complete) &&
+           sym_versioned(h, "nvJitLinkGetLinkedCubinSize", a.cubin_size) &&
+           sym_versioned(h, "nvJitLinkGetLinkedCubin", a.cubin) &&
+           sym_versioned(h, "nvJitLinkGetErrorLogSize", a.log_size) &&
+           sym_versioned(h, "nvJitLinkGetErrorLog", a.log) && sym_versioned(h, "nvJitLinkDestroy", a.destroy);
+    if (!a.ok) s.last_log = "nvJitLink (libnvJitLink.so.12) is not available";
+    return a.ok;
+}
+
 // Compile `e` (no lock held while NVRTC runs).
 void compile_entry(State& s, Entry& e) {
     auto t0 = std::chrono::steady_clock::now();
@@ -154,6 +212,7 @@ void compile_entry(State& s, Entry& e) {
             }
         }
         std::vector<const char*> opts = {"-arch=sm_100a", "-std=c++17", "-w"};
+        if (e.rdc) opts.push_back("-rdc=true");
         for (const auto& x : extra) opts.push_back(x.c_str());
         nvrtcResult r = a.compile(prog, int(opts.size()), opts.data());
         size_t ls = 0;
@@ -345,6 +404,156 @@ void* lookup(const std::string& src, const char* name, bool block, bool load, in
     std::lock_guard<std::mutex> lock(s.mu);
     if (e->state != 1) return nullptr;
     return device_function(s, *e, load, threads, smem, occ);
+}
+
+std::string queue_device_fn(const std::string& src, const char* name) {
+    State& s = S();
+    std::unique_lock<std::mutex> lock(s.mu);
+    if (!load_nvrtc(s)) return std::string();
+    const std::string key = source_key(src) + "r";
+    if (s.cache.find(key) != s.cache.end()) return key;
+    if (s.stopping) return std::string();
+    auto e = std::make_shared<Entry>();
+    e->src = src;
+    e->name = name;
+    e->rdc = true;
+    s.cache.emplace(key, e);
+    ++s.pending;
+    start_workers(s);
+    s.queue.push_back(e);
+    s.cv.notify_all();
+    return key;
+}
+
+// The linked cubin of `base`, the dispatcher and the compiled functions
+// `keys` (empty on failure, with last_log set).  block: wait for the
+// functions' compilations; otherwise fail while any is pending.
+std::string link_cubin(const void* base, size_t base_size, const std::string& dispatcher,
+                       const std::vector<std::string>& keys, bool block) {
+    State& s = S();
+    std::vector<std::shared_ptr<Entry>> es;
+    {
+        std::unique_lock<std::mutex> lock(s.mu);
+        if (!load_nvrtc(s)) return std::string();
+        for (const auto& k : keys) {
+            auto e = s.cache.find(k);
+            if (e == s.cache.end()) {
+                s.last_log = "link: a device function was never queued";
+                return std::string();
+            }
+            es.push_back(e->second);
+        }
+        auto all_done = [&] {
+            for (const auto& e : es)
+                if (e->state == 0) return false;
+            return true;
+        };
+        if (block) s.cv.wait(lock, all_done);
+        if (!all_done()) {
+            s.last_log = "link: device functions still compiling";
+            return std::string();
+        }
+        for (const auto& e : es)
+            if (e->state != 1) {
+                s.last_log = "link: compile of " + e->name + " failed: " + e->log.substr(0, 3000);
+                return std::string();
+            }
+        if (!load_link(s)) return std::string();
+        ++s.pending;  // the dispatcher, compiled below
+    }
+    Entry d;
+    d.src = dispatcher;
+    d.name = "qs_batch_dispatch";
+    d.rdc = true;
+    compile_entry(s, d);
+    if (d.state != 1) {
+        std::lock_guard<std::mutex> lock(s.mu);
+        s.last_log = "link: compile of the dispatcher failed: " + d.log.substr(0, 3000);
+        return std::string();
+    }
+    LinkApi& L = s.link;
+    nvJitLinkHandle h = nullptr;
+    const char* lopts[] = {"-arch=sm_100a"};
+    std::string err;
+    bool ok = L.create(&h, 1, lopts) == NVJITLINK_SUCCESS;
+    if (ok) ok = L.add(h, NVJITLINK_INPUT_CUBIN, base, base_size, "batch_kernel") == NVJITLINK_SUCCESS;
+    if (ok) ok = L.add(h, NVJITLINK_INPUT_CUBIN, d.cubin.data(), d.cubin.size(), "dispatch") == NVJITLINK_SUCCESS;
+    for (size_t i = 0; ok && i < es.size(); ++i)  // ready entries' cubins no longer change
+        ok = L.add(h, NVJITLINK_INPUT_CUBIN, es[i]->cubin.data(), es[i]->cubin.size(), es[i]->name.c_str()) ==
+             NVJITLINK_SUCCESS;
+    if (ok) ok = L.complete(h) == NVJITLINK_SUCCESS;
+    std::string cubin;
+    size_t cs = 0;
+    if (ok) ok = L.cubin_size(h, &cs) == NVJITLINK_SUCCESS && cs > 0;
+    if (ok) {
+        cubin.resize(cs);
+        ok = L.cubin(h, &cubin[0]) == NVJITLINK_SUCCESS;
+    }
+    if (!ok && h) {
+        size_t ls = 0;
+        if (L.log_size(h, &ls) == NVJITLINK_SUCCESS && ls > 1) {
+            err.resize(ls);
+            L.log(h, &err[0]);
+        }
+    }
+    if (h) L.destroy(&h);
+    if (!ok) {
+        std::lock_guard<std::mutex> lock(s.mu);
+        s.last_log = "nvJitLink failed: " + err.substr(0, 4000);
+        return std::string();
+    }
+    return cubin;
+}
+
+void* link_module(uint64_t link_key, const void* base, size_t base_size, const std::string& dispatcher,
+                  const std::vector<std::string>& keys, const char* kernel, bool block, bool load, int threads,
+                  size_t smem, int* occ) {
+    State& s = S();
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::shared_ptr<Linked> lm;
+    {
+        std::lock_guard<std::mutex> lock(s.mu);
+        auto it = s.linked.find(link_key);
+        if (it != s.linked.end() && it->second->fn[dev]) {
+            *occ = it->second->occ[dev];
+            return it->second->fn[dev];
+        }
+        if (!load || !load_driver(s)) return nullptr;
+        if (it == s.linked.end()) it = s.linked.emplace(link_key, std::make_shared<Linked>()).first;
+        lm = it->second;
+    }
+    const std::string cubin = link_cubin(base, base_size, dispatcher, keys, block);
+    if (cubin.empty()) return nullptr;
+    std::lock_guard<std::mutex> lock(s.mu);
+    cudaFree(nullptr);  // the runtime's primary context is current from here on
+    CUmodule mod = nullptr;
+    CUresult r = s.api.module_load(&mod, cubin.data());
+    if (r != CUDA_SUCCESS) {
+        const char* m = nullptr;
+        s.api.cu_err(r, &m);
+        s.last_log = std::string("cuModuleLoadData (linked batch kernel): ") + (m ? m : "error");
+        return nullptr;
+    }
+    CUfunction fn = nullptr;
+    if (s.api.get_function(&fn, mod, kernel) != CUDA_SUCCESS) {
+        s.last_log = std::string("cuModuleGetFunction failed for ") + kernel;
+        return nullptr;
+    }
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // the kernel's static shared memory (a few hundred bytes) comes out of the same opt-in limit
+    if (optin > 4096) s.api.set_attr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, optin - 4096);
+    int nb = 0;
+    if (s.api.occupancy(&nb, fn, threads, smem) != CUDA_SUCCESS || nb < 1) {
+        s.last_log = "cuOccupancyMaxActiveBlocksPerMultiprocessor: the linked batch kernel does not fit an SM";
+        return nullptr;
+    }
+    lm->mod[dev] = mod;
+    lm->fn[dev] = fn;
+    lm->occ[dev] = nb;
+    *occ = nb;
+    return fn;
 }
 
 int launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st, void** params) {

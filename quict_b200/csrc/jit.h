@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -27,6 +28,28 @@ void set_mode(int m);
 // blocks per SM at `threads` threads and `smem` dynamic shared memory
 // (computed when the kernel is loaded).
 void* lookup(const std::string& src, const char* name, bool block, bool load, int threads, size_t smem, int* occ);
+
+// Queue the compilation of `src` as relocatable device code (NVRTC -rdc,
+// defining the extern "C" __device__ function `name`); returns its cache key
+// ("" when NVRTC is unavailable or the compiler is shut down).
+std::string queue_device_fn(const std::string& src, const char* name);
+
+// The cubin link_module would load (no device needed): `base` linked with the
+// dispatcher (compiled here) and the compiled functions `keys`; empty on
+// failure (last_log says why).  block: wait for the functions' compilations.
+std::string link_cubin(const void* base, size_t base_size, const std::string& dispatcher,
+                       const std::vector<std::string>& keys, bool block);
+
+// Link the relocatable cubin `base` (the batch kernel), the `dispatcher`
+// source (compiled here) and the queued device functions `keys` with
+// nvJitLink into one module, load it on the current device and return its
+// kernel `kernel` (cached under link_key per device); *occ <- resident blocks
+// per SM at `threads` threads and `smem` dynamic shared memory.  block: wait
+// for the queued compilations; load == false (stream capture): only an
+// already linked kernel is returned.  Null on failure (last_log says why).
+void* link_module(uint64_t link_key, const void* base, size_t base_size, const std::string& dispatcher,
+                  const std::vector<std::string>& keys, const char* kernel, bool block, bool load, int threads,
+                  size_t smem, int* occ);
 
 // cuLaunchKernel of a looked-up function; `params` points to the kernel's
 // parameter values (one pointer per kernel argument).

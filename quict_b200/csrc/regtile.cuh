@@ -1134,4 +1134,14 @@ int build_reg(const qs_pass& ps, const qs_op* ops, std::vector<int>& rem, int n,
 }
 
 }  // namespace
+
+// Generated source of a planned register pass (`regargs`: a RegArgs filled by
+// build_reg; the struct has the same layout in every file that includes this
+// header) as the `extern "C" __device__` function `name` called by the
+// linked persistent batch kernel; its parameter block, dynamic shared memory
+// and thread count.  mats_host: the host matrix table in the state's
+// precision.  False when the pass is not generated (fused.cu).
+bool gen_batch_pass(const void* regargs, int R, bool c128, const void* mats_host, const char* name, std::string* src,
+                    std::vector<uint64_t>* params, size_t* smem, int* threads);
+
 }  // namespace qs

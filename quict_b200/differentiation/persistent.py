@@ -50,7 +50,7 @@ class PersistentBatch:
 
     def __init__(self, problems: Sequence[Tuple[BatchedAdjoint, np.ndarray]], precision: str = "single",
                  device_id: int = 0, caps: Optional[Tuple[int, int]] = None, tiles_per_item: int = 16,
-                 amps_per_ham_item: int = 1 << 14, timeout_s: float = 10.0):
+                 amps_per_ham_item: int = 1 << 14, timeout_s: float = 10.0, jit_min_qubits: int = 20):
         if not problems:
             raise ValueError("an empty batch")
         self.dev = require_cuda(device_id)
@@ -123,7 +123,9 @@ class PersistentBatch:
         wa = np.array(ws if ws else [0.0], dtype=np.float64)
         sizes = N.qs_batch_sizes()
         offs = (C.c_int64 * len(problems))()
+        self.jit_min_qubits = jit_min_qubits
         args = (self.dtype, insts, len(problems), cpass, len(passes), cop, len(ops), host.size,
+                C.c_void_p(host.ctypes.data) if host.size else None, int(jit_min_qubits),
                 xa.ctypes.data_as(C.c_void_p), za.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p), len(xa),
                 wa.ctypes.data_as(C.c_void_p), len(ws), int(tiles_per_item), int(amps_per_ham_item))
         N.call("qs_batch_plan", *args, None, 0, C.byref(sizes), offs)
@@ -143,22 +145,31 @@ class PersistentBatch:
         self.ctrl = torch.zeros(int(sizes.ctrl_bytes) // 8, dtype=torch.int64, device=dev)
         self.graph = None
         self.launches = 0
+        self.linked = False
 
     # ---- running -------------------------------------------------------------------
-    def launch(self, stream=None) -> None:
-        """Issue the batch (control-word memset + one kernel) on `stream`."""
+    def launch(self, stream=None) -> bool:
+        """Issue the batch (control-word memset + one kernel) on `stream`;
+        True when the kernel linked with the generated stage functions ran,
+        False for the generic one."""
         st = N.stream_ptr(stream if stream is not None else torch.cuda.current_stream(self.dev))
-        N.call("qs_batch_launch", C.byref(self.sizes), C.c_void_p(self.blob.data_ptr()),
+        rc = N.call("qs_batch_launch", C.byref(self.sizes), C.c_void_p(self.blob.data_ptr()),
                C.c_void_p(self.states.data_ptr()), C.c_void_p(self.mats.data_ptr()),
                C.c_void_p(self.partials.data_ptr()), C.c_void_p(self.energies.data_ptr()),
                C.c_void_p(self.grads.data_ptr()), C.c_void_p(self.ctrl.data_ptr()), self.ctrl.numel() * 8,
                self.timeout_s, st)
         self.launches += 1
+        self.linked = rc == 1
+        return self.linked
 
     def capture(self) -> "torch.cuda.CUDAGraph":
-        """One eager run (kernel configuration happens outside capture), then
-        the launch captured into a CUDA graph."""
+        """Eager runs first (the generated stage functions finish compiling
+        and the linked kernel is loaded outside capture), then the launch
+        captured into a CUDA graph."""
         self.launch()
+        if self.sizes.jit_fns > 0:
+            N.jit_wait(1800)
+            self.launch()
         torch.cuda.synchronize(self.dev)
         self.check()
         self.graph = torch.cuda.CUDAGraph()
@@ -208,9 +219,7 @@ def tune(make_batch, precision: str, key: Optional[str] = None, tuner: Optional[
     best, best_ms = None, math.inf
     for caps in CAP_CANDIDATES[precision]:
         b = make_batch(caps)
-        b.launch()
-        torch.cuda.synchronize(b.dev)
-        b.check()
+        b.capture()  # compiles and links the generated stage functions, if any
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
         for _ in range(reps):

@@ -92,7 +92,8 @@ class UnevenQAOABatch:
             self.engines = [BatchedAdjoint(qaoa_circuit(n, edges, p), maxcut_observable(n, edges), precision,
                                            device_id) for n, edges, p, _ in instances]
             self.persistent = PersistentBatch([(e, np.asarray(prm)) for e, (_, _, _, prm) in
-                                               zip(self.engines, instances)], precision, device_id, caps=self.caps)
+                                               zip(self.engines, instances)], precision, device_id, caps=self.caps,
+                                              jit_min_qubits=jit_min_qubits)
             self.caps = self.persistent.caps
             self.dev = self.persistent.dev
             return
@@ -132,9 +133,10 @@ class UnevenQAOABatch:
         probs = [(e, np.asarray(prm)) for e, (_, _, _, prm) in zip(self.engines, self.instances)]
         key = batch_key(torch.cuda.get_device_name(self.dev), prec, label)
         self.persistent = None
-        best, ms, trials = tune(lambda caps: PersistentBatch(probs, prec, self.dev.index, caps=caps), prec, key,
-                                tuner)
-        self.persistent = PersistentBatch(probs, prec, self.dev.index, caps=best)
+        jm = self.jit_min_qubits
+        best, ms, trials = tune(lambda caps: PersistentBatch(probs, prec, self.dev.index, caps=caps,
+                                                             jit_min_qubits=jm), prec, key, tuner)
+        self.persistent = PersistentBatch(probs, prec, self.dev.index, caps=best, jit_min_qubits=jm)
         self.caps = best
         self.graph = None
         return best, ms, trials

@@ -46,6 +46,8 @@ def test_persistent_c64_matches_per_instance_c128_up_to_24_qubits(cuda_ok):
     torch.cuda.synchronize()
     res = batch.results()
     assert batch.captured_launches == 1
+    # the problems of >= 20 qubits run as generated functions in the linked kernel
+    assert batch.persistent.sizes.jit_fns > 0 and batch.persistent.linked
     for (n, edges, p, _), (e, g), (e2, g2) in zip(inst, res, _reference(inst)):
         scale = max(1.0, len(edges))
         assert abs(e - e2) < 1e-5 * scale, (n, p, e, e2)
@@ -161,10 +163,12 @@ def _tiny_plan_args(n=10, nterms=2, nslots=1, nparams=1, k=10, bwd_k=10, pair=No
     return inst, passes, ops, x, z, c, w
 
 
-def _plan(inst, passes, ops, x, z, c, w, tiles=4, amps=4096, blob=None, nbytes=0, mats=4):
+def _plan(inst, passes, ops, x, z, c, w, tiles=4, amps=4096, blob=None, nbytes=0, mats=4, mats_host=None,
+          jit_min_qubits=99):
     sizes = N.qs_batch_sizes()
     lib = N.load()
-    rc = lib.qs_batch_plan(N.QS_C64, inst, len(inst), passes, len(passes), ops, len(ops), mats,
+    rc = lib.qs_batch_plan(N.QS_C64, inst, len(inst), passes, len(passes), ops, len(ops), mats, mats_host,
+                           jit_min_qubits,
                            x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
                            c.ctypes.data_as(C.c_void_p), len(x), w.ctypes.data_as(C.c_void_p), len(w), tiles, amps,
                            blob, nbytes, C.byref(sizes), None)
@@ -210,3 +214,23 @@ def test_planner_rejects_bad_batches(bad):
         args[1][1].pair = 3  # the pair bit of a backward pass must be bit n
     rc, _ = _plan(*args, **extra)
     assert rc < 0
+
+
+def test_generated_stage_functions_compile_and_link_without_a_device():
+    """With the host matrix table, the planner generates the register stages
+    as device functions; they compile (NVRTC, relocatable) and link with the
+    embedded batch kernel (nvJitLink) here, with torch imported first (it
+    brings its own, older libnvJitLink)."""
+    import torch  # noqa: F401
+    args = _tiny_plan_args()
+    mats = np.array([1, 1j, 1, -1], dtype=np.complex64)
+    rc, sz = _plan(*args, mats_host=C.c_void_p(mats.ctypes.data), jit_min_qubits=0)
+    assert rc == 0 and sz.jit_fns == 2 and sz.jit_key != 0
+    blob = np.zeros(int(sz.blob_bytes), dtype=np.uint8)
+    rc, sz = _plan(*args, blob=blob.ctypes.data_as(C.c_void_p), nbytes=blob.nbytes,
+                   mats_host=C.c_void_p(mats.ctypes.data), jit_min_qubits=0)
+    assert rc == 0
+    nb = C.c_int64()
+    rc = N.load().qs_batch_link_check(C.byref(sz), C.byref(nb))
+    assert rc == 0, N.load().qs_last_error()
+    assert nb.value > 0
