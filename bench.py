@@ -13,7 +13,8 @@ value   gates/s with the state resident in HBM, device-timed (CUDA events),
 e2e     the same metric through the public API (StateVectorSimulator.run):
         host planning, matrix-table host->device copy and a device->host read
         of P(qubit 0 = 0) inside every step.
-roofline  the fused-pass kernel (k_fused_reg), bound fp64: algorithmic flops of
+roofline  the fused-pass kernel (qs_pass: each pass compiled at run time; the
+        generic k_fused_reg runs a pass until its kernel is ready), bound fp64: algorithmic flops of
         its ops over its CUDA-event time, against cuBLAS DGEMM measured here;
         roofline_hbm: 2 * 2^n * 16 bytes per launch against MEASURED_PEAKS.json.
 single_gate_sweep, c64, configs_0_2, adjoint, qaoa  extra sections: per-gate HBM
@@ -53,13 +54,16 @@ def peaks():
 
 
 def ncu_traffic(n):
-    """dram bytes per fused-pass launch from the committed ncu summary (a
-    26-qubit capture scaled by the amplitudes processed), or None."""
-    p = os.path.join(ROOT, "profiles", "k_fused_reg_config1_c128.txt")
-    if not os.path.exists(p):
-        return None
-    m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) * 2.0 ** (n - 30) if m else None
+    """dram bytes per fused-pass launch from the committed ncu summary of the
+    generated pass kernel (a 26-qubit capture scaled by the amplitudes
+    processed), or None."""
+    for name in ("qs_pass_config1_c128.txt", "k_fused_reg_config1_c128.txt"):
+        p = os.path.join(ROOT, "profiles", name)
+        if os.path.exists(p):
+            m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", open(p).read())
+            if m:
+                return float(m.group(1)) * 2.0 ** (n - 30)
+    return None
 
 
 class Clocks:
@@ -392,26 +396,48 @@ def grad_bench(ws, rank, local, batch=1024):
     return out
 
 
-def qaoa_bench(ws, rank, local, count=512):
-    """Config 4: uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6), one CUDA
-    graph per rank (instances split over ranks by amplitude x depth cost), complex64."""
+def qaoa_bench(ws, rank, local, count=512, graph_too=False):
+    """Config 4: uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6),
+    complex64, instances split over ranks by amplitude x depth cost.  Timed:
+    ONE persistent launch per rank (qs_batch_launch: every instance's forward
+    passes, lam = C psi, energy, adjoint sweep and sums as work items; the
+    register stages of instances >= 22 qubits as generated functions linked
+    into the kernel), replayed from a CUDA graph (a control-word memset node
+    and the kernel node).  graph_too: also the per-instance kernel chains
+    captured over 16 streams into one graph, for comparison."""
     import torch
     from quict_b200.differentiation import UnevenQAOABatch, qaoa_instances
     from quict_b200.distributed import balanced_shard
     inst = qaoa_instances(count)
     parts = balanced_shard([float(2 ** n) * (p * (1.5 * n + n)) for n, _, p, _ in inst], ws)
     mine = [inst[i] for i in parts[rank]]
+    total_grads = sum(2 * p for _, _, p, _ in inst)
+    out = {"workload": f"qaoa-maxcut-{count}instances-n10..24-p1..6", "dtype": "c64"}
     t0 = time.perf_counter()
-    batch = UnevenQAOABatch(mine, "single", local)
+    batch = UnevenQAOABatch(mine, "single", local, mode="persistent", label=f"qaoa{count}")
     batch.capture()
     setup_s = time.perf_counter() - t0
     barrier(ws)
     ms = max_over_ranks(_events_ms(batch.replay, 3), ws)
-    total_grads = sum(2 * p for _, _, p, _ in inst)
-    return {"workload": f"qaoa-maxcut-{count}instances-n10..24-p1..6", "graph_replay_ms": ms,
-            "grads_per_s": total_grads / (ms / 1e3), "instances_per_s": count / (ms / 1e3),
-            "launches_per_replay": batch.captured_launches, "setup_s_incl_compile": setup_s,
-            "jit_min_qubits": batch.jit_min_qubits}
+    batch.persistent.check()
+    sz = batch.persistent.sizes
+    out.update({"graph_replay_ms": ms, "grads_per_s": total_grads / (ms / 1e3), "instances_per_s": count / (ms / 1e3),
+                "launches_per_replay": 1, "graph_nodes": "memset of the control words + the persistent kernel",
+                "linked_generated_stages": bool(batch.persistent.linked), "generated_functions": int(sz.jit_fns),
+                "work_items": int(sz.nitems), "cta_threads": int(sz.threads), "caps": list(batch.caps),
+                "jit_min_qubits": batch.jit_min_qubits, "setup_s_incl_compile_and_link": setup_s})
+    del batch
+    torch.cuda.empty_cache()
+    if graph_too:
+        t0 = time.perf_counter()
+        g = UnevenQAOABatch(mine, "single", local, mode="graph")
+        g.capture()
+        setup_s = time.perf_counter() - t0
+        barrier(ws)
+        gms = max_over_ranks(_events_ms(g.replay, 3), ws)
+        out["per_instance_chains"] = {"graph_replay_ms": gms, "launches_per_replay": g.captured_launches,
+                                      "setup_s_incl_compile": setup_s}
+    return out
 
 
 def small_configs_bench(ws, local, reps=3):
@@ -710,13 +736,13 @@ def run_ours(args, ws, rank, local):
                    "l2": f"inputs larger than L2 ({(1 << n) * 16 / 2**30:g} GiB state vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "hbm_gbs_effective": npasses * bytes_per_pass / (ms / 1e3) / 1e9,
-        "roofline": {"bound": "fp64", "kernel": "k_fused_reg", "achieved": fp64_achieved, "peak": fp64_peak,
+        "roofline": {"bound": "fp64", "kernel": "qs_pass", "achieved": fp64_achieved, "peak": fp64_peak,
                      "unit": "TFLOP/s", "frac": fp64_achieved / fp64_peak, "peak_source": fp64_src,
                      "traffic": ncu_traffic(n), "algorithmic_flops_per_launch": flops / max(1, len(pass_list)),
                      "avg_launch_ms": avg_pass_ms,
                      "note": "a fused pass applies ~20 merged ops per HBM round trip, so FP64 issue, not HBM, "
                              "bounds it; roofline_hbm gives the HBM view"},
-        "roofline_hbm": {"bound": "hbm", "kernel": "k_fused_reg", "achieved": achieved, "peak": peak,
+        "roofline_hbm": {"bound": "hbm", "kernel": "qs_pass", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(n),
                          "algorithmic_bytes_per_launch": bytes_per_pass, "avg_launch_ms": avg_pass_ms},
         "e2e": {"value": ws * len(ops) / e2e_s, "unit": "gates/s", "h2d_bytes_per_step": int(h2d),
@@ -746,7 +772,7 @@ def run_ours(args, ws, rank, local):
         line["configs_0_2"] = small_configs_bench(ws, local)
     if not args.no_grad:
         line["adjoint"] = grad_bench(ws, rank, local)
-        line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances)
+        line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances, graph_too=args.qaoa_graph)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         torch.cuda.empty_cache()
         cb = CpuBaseline(circuit, n)
@@ -786,6 +812,8 @@ def main():
                     help="gate-merging block width (0 disables; default: the tuning cache)")
     ap.add_argument("--no-extra", action="store_true", help="skip the complex64 30q / 32q runs")
     ap.add_argument("--qaoa-instances", type=int, default=512)
+    ap.add_argument("--qaoa-graph", action="store_true",
+                    help="also time config 4 as per-instance kernel chains in one CUDA graph")
     ap.add_argument("--max-pass-cost", type=float, default=None,
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units (default: the tuning cache)")
     ap.add_argument("--jit", type=int, default=1,

@@ -116,6 +116,9 @@ def main() -> None:
 
         python -m quict_b200.workloads gradient --batch 256 [--precision single] [--repeat 2]
             [--tile-bits K] [--pair-tile-bits K]                       (cuda:0)
+        python -m quict_b200.workloads qaoa-batch --instances 8 --sizes 20,22,24 [--repeat 2]
+            [--tiles-per-item T] [--tile-bits K] [--pair-tile-bits K]  (cuda:0; ONE persistent
+            launch per repeat, after the warm-up run that compiles and links its stages)
         torchrun --nproc-per-node N -m quict_b200.workloads sharded --qubits Q
             [--precision double] [--gates 1000]                        (one GPU per rank)
     """
@@ -126,7 +129,10 @@ def main() -> None:
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["gradient", "sharded"])
+    ap.add_argument("workload", choices=["gradient", "sharded", "qaoa-batch"])
+    ap.add_argument("--instances", type=int, default=8)
+    ap.add_argument("--sizes", default="20,22,24", help="qubit counts of the seeded QAOA instances")
+    ap.add_argument("--tiles-per-item", type=int, default=16)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--precision", default=None, choices=["single", "double"])
     ap.add_argument("--repeat", type=int, default=2)
@@ -149,6 +155,21 @@ def main() -> None:
             dist.destroy_process_group()
         return
     a.precision = a.precision or "single"
+    if a.workload == "qaoa-batch":
+        from .differentiation import BatchedAdjoint, maxcut_observable, qaoa_circuit, qaoa_instances
+        from .differentiation.persistent import DEFAULT_CAPS, PersistentBatch
+        inst = qaoa_instances(a.instances, sizes=tuple(int(v) for v in a.sizes.split(",")))
+        caps = (a.tile_bits or DEFAULT_CAPS[a.precision][0], a.pair_tile_bits or DEFAULT_CAPS[a.precision][1])
+        pb = PersistentBatch([(BatchedAdjoint(qaoa_circuit(n, e, p), maxcut_observable(n, e), a.precision), prm)
+                              for n, e, p, prm in inst], a.precision, caps=caps, tiles_per_item=a.tiles_per_item,
+                             jit_min_qubits=min(int(v) for v in a.sizes.split(",")))
+        pb.capture()
+        for _ in range(a.repeat):
+            pb.launch()
+        res = pb.results()
+        print(f"qaoa batch {a.instances} {a.precision}: linked={pb.linked} items={pb.sizes.nitems} "
+              f"sum E = {sum(e for e, _ in res):.6e}")
+        return
     from .differentiation import BatchedAdjoint
     circ, obs, params = config3_problem(16, 8, a.batch)
     eng = BatchedAdjoint(circ, obs, a.precision, tile_bits=a.tile_bits, pair_tile_bits=a.pair_tile_bits)
