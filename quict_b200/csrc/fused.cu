@@ -325,6 +325,16 @@ int launch_smem(V* vec, V* vec2, int n, const qs_pass& ps, const qs_op* ops, con
 // depends on the pass's structure and on which matrix entries are exactly
 // 0, 1 or -1, not on the other matrix values, so passes of the same shape
 // share one compiled kernel (jit.cu caches by source text).
+// Single-buffered generated kernels (see gen_reg_pass): QS_JIT_SINGLE_BUFFER=0 / 1,
+// else complex128 only.
+inline bool jit_single_buffer(bool c128) {
+    static const int env = [] {
+        const char* e = getenv("QS_JIT_SINGLE_BUFFER");
+        return e && (*e == '0' || *e == '1') ? *e - '0' : -1;
+    }();
+    return env >= 0 ? env == 1 : c128;
+}
+
 struct JitPass {
     std::string src;
     std::vector<uint64_t> params;  // the kernel's parameter block (16-byte multiple)
@@ -525,8 +535,17 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
         return "p.m[" + std::to_string(int(a.ops[o].moff)) + " + ";
     };
     const unsigned hoff_n = (1u << H) < 2u ? 2u : (1u << H);  // a 16-byte multiple
+    // One tile buffer instead of two (kernels only): the next tile is fetched
+    // after this one's stores, and the smaller footprint lets more CTAs share
+    // an SM, whose loads and arithmetic overlap.  Measured on the 30-qubit
+    // config-1 circuit (B200): complex128 k = 10 316.7 -> 297.5 ms (8 instead of
+    // 6 CTAs per SM), complex64 k = 11 213.6 -> 226.8 ms; so the default is
+    // single for complex128 and double for complex64.  QS_JIT_SINGLE_BUFFER=0/1
+    // overrides it.
+    const bool single = devfn == nullptr && jit_single_buffer(C128);
+    const int nbuf = single ? 1 : 2;
     out.threads = threads;
-    out.smem = sizeof(V) * 2 * (size_t(1) << K) + 8 * size_t(hoff_n) +
+    out.smem = sizeof(V) * size_t(nbuf) * (size_t(1) << K) + 8 * size_t(hoff_n) +
                (a.nexp > 0 ? sizeof(double2) * size_t(nwarps) * size_t(a.nexp) : 0) +
                (batched ? sizeof(V) * size_t(NM) : 0) + sizeof(V) * size_t(ndsm);
     if (!with_source) return true;
@@ -577,7 +596,7 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
               minb);
     }
     g.add("  extern __shared__ __align__(16) unsigned char smem_raw[];\n");
-    g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", 1u << K);
+    g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", single ? 0u : 1u << K);
     g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
     g.add("  double2* const ered = reinterpret_cast<double2*>(hoff + %du);\n", hoff_n);
     g.add("  V* const msm = reinterpret_cast<V*>(ered + %d);\n", a.nexp > 0 ? nwarps * a.nexp : 0);
@@ -637,7 +656,7 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     g.add("  for (u32 it = 0; tile < tend; ++it, tile += tstep) {\n");
     g.add("    V* const cur = (it & 1u) ? b1 : b0;\n    const u64 base = tile_base(tile);\n");
     g.add("    asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n    __syncthreads();\n");
-    g.add("    if (tile + tstep < tend) prefetch((it & 1u) ? b0 : b1, tile_base(tile + tstep));\n");
+    if (!single) g.add("    if (tile + tstep < tend) prefetch((it & 1u) ? b0 : b1, tile_base(tile + tstep));\n");
     if (batched) {
         g.add("    { const u64 inst = (base & p.misc[0]) >> p.misc[1];\n");
         g.add("      if (inst != staged) {\n");
@@ -841,6 +860,8 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
         g.add("      const u64 at = 2 * (p.eslot[e] * ntiles + tile);\n      partials[at] = t.x;\n"
               "      partials[at + 1] = t.y; }\n");
     }
+    if (single)  // every thread is past its last read of the buffer
+        g.add("    __syncthreads();\n    if (tile + tstep < tend) prefetch(b0, tile_base(tile + tstep));\n");
     g.add("  }\n}\n");
     if (g.truncated) return false;
     out.src.swap(g.s);
@@ -887,6 +908,8 @@ uint64_t plan_key(const RegArgs& a, int R, size_t vsize, const std::vector<uint8
         return e && *e ? atoi(e) : 0;
     }();
     h = fnv(h, &target, sizeof(target));
+    const int single = jit_single_buffer(vsize == 16) ? 1 : 0;
+    h = fnv(h, &single, sizeof(single));
     return fnv(h, classes.data(), classes.size());
 }
 
