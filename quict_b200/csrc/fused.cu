@@ -548,6 +548,11 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     out.smem = sizeof(V) * size_t(nbuf) * (size_t(1) << K) + 8 * size_t(hoff_n) +
                (a.nexp > 0 ? sizeof(double2) * size_t(nwarps) * size_t(a.nexp) : 0) +
                (batched ? sizeof(V) * size_t(NM) : 0) + sizeof(V) * size_t(ndsm);
+    out.smem = (out.smem + 15) & ~size_t(15);
+    // a device function keeps its parameter block in shared memory behind the
+    // rest (see its prologue); the kernels read theirs from the parameter bank
+    const size_t smem_main = out.smem;
+    if (devfn) out.smem += 8 * out.params.size();
     if (!with_source) return true;
     const char* VT = C128 ? "double2" : "float2";
     const char* ST = C128 ? "double" : "float";
@@ -589,13 +594,23 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     if (devfn) {
         g.add("extern \"C\" __device__ void %s(V* __restrict__ vec, const void* __restrict__ pv, "
               "const V* __restrict__ mats, double* __restrict__ partials, u64 tile, const u64 tend, "
-              "const u32 zero_in) {\n  const P& p = *reinterpret_cast<const P*>(pv);\n", devfn);
+              "const u32 zero_in) {\n", devfn);
     } else {
         g.add("extern \"C\" __global__ void __launch_bounds__(%d, %d) qs_pass(V* __restrict__ vec, "
               "const __grid_constant__ P p, const V* __restrict__ mats, double* __restrict__ partials) {\n", threads,
               minb);
     }
     g.add("  extern __shared__ __align__(16) unsigned char smem_raw[];\n");
+    if (devfn) {
+        // the parameter block moves from the plan (global memory) to shared
+        // memory behind the tile buffers: matrix entries are read at shared-
+        // memory latency, as the kernels read them from the constant bank
+        g.add("  { const uint4* __restrict__ src = reinterpret_cast<const uint4*>(pv);\n"
+              "    uint4* dst = reinterpret_cast<uint4*>(smem_raw + %zuu);\n"
+              "    for (u32 i = threadIdx.x; i < %zuu; i += blockDim.x) dst[i] = src[i]; }\n"
+              "  __syncthreads();\n  const P& p = *reinterpret_cast<const P*>(smem_raw + %zuu);\n",
+              smem_main, out.params.size() / 2, smem_main);
+    }
     g.add("  V* const b0 = reinterpret_cast<V*>(smem_raw);\n  V* const b1 = b0 + %du;\n", single ? 0u : 1u << K);
     g.add("  u64* const hoff = reinterpret_cast<u64*>(b1 + %du);\n", 1u << K);
     g.add("  double2* const ered = reinterpret_cast<double2*>(hoff + %du);\n", hoff_n);
