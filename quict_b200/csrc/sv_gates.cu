@@ -272,6 +272,113 @@ k_1q_shfl(V* __restrict__ v, uint64_t chunks, Plan plan_hi, uint64_t cmask_hi, u
     }
 }
 
+// ------------------------------------------- 1q, controls among the low bits
+// Target bit < 5 with controls below bit 5: the lanes walk the 5 lowest bits
+// that are not controls (lanemask) and every control bit is fixed to 1, so a
+// warp loads and stores only amplitudes the gate changes (the chunk kernels
+// above load the whole 32- or 64-amplitude chunk and store the lanes whose
+// controls are set: 1.5x the bytes for one control).  r: the target's
+// position among the lane bits; its partner is lane ^ 2^r.
+__device__ __forceinline__ uint64_t lane_offset(int lane, uint64_t lanemask) {
+    uint64_t o = 0;
+    for (int i = 0, b = 0; i < 5; ++b)
+        if ((lanemask >> b) & 1) {
+            if ((lane >> i) & 1) o |= uint64_t(1) << b;
+            ++i;
+        }
+    return o;
+}
+
+template <typename V, int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_1q_lanes(V* __restrict__ v, uint64_t chunks, Plan plan, uint64_t cmask, uint64_t lanemask, int r, Mat<V, 4> M) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (kThreads / 32);
+    const uint64_t w0 = uint64_t(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+    const uint64_t loff = lane_offset(lane, lanemask) | cmask;
+    const bool one = (lane >> r) & 1;
+    for (uint64_t c0 = w0; c0 < chunks; c0 += warps * kUnroll) {
+        V a[kUnroll];
+        uint64_t idx[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c < chunks) {  // warp-uniform
+                idx[u] = expand(c, plan) | loff;
+                a[u] = v[idx[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c >= chunks) continue;
+            const V p = shfl_xor(a[u], 1 << r);
+            V out;
+            if (KIND == QS_K_DENSE) out = one ? cfma(M.m[2], p, cmul(M.m[3], a[u])) : cfma(M.m[0], a[u], cmul(M.m[1], p));
+            else out = one ? cmul(M.m[2], p) : cmul(M.m[1], p);
+            v[idx[u]] = out;
+        }
+    }
+}
+
+// complex64 form with 128-bit accesses (bit 0 is not a control): each lane
+// moves the amplitude pair (bit 0 = 0, 1) as a float4; the lanes walk the 5
+// lowest non-control bits above bit 0.  A target on bit 0 is the lane's own
+// pair; any other target's partner is lane ^ 2^r.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_1q_lanes_v2(float2* __restrict__ v, uint64_t chunks, Plan plan, uint64_t cmask, uint64_t lanemask, int bit, int r,
+              Mat<float2, 4> M) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (kThreads / 32);
+    const uint64_t w0 = uint64_t(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+    float4* __restrict__ v4 = reinterpret_cast<float4*>(v);
+    const uint64_t loff = lane_offset(lane, lanemask) | cmask;
+    const bool one = bit > 0 && ((lane >> r) & 1);
+    for (uint64_t c0 = w0; c0 < chunks; c0 += warps * kUnroll) {
+        float4 a[kUnroll];
+        uint64_t q[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c < chunks) {  // warp-uniform
+                q[u] = (expand(c, plan) | loff) >> 1;
+                a[u] = v4[q[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t c = c0 + uint64_t(u) * warps;
+            if (c >= chunks) continue;
+            const float2 x0 = make_float2(a[u].x, a[u].y), x1 = make_float2(a[u].z, a[u].w);
+            float2 y0, y1;
+            if (bit == 0) {
+                if (KIND == QS_K_DENSE) {
+                    y0 = cfma(M.m[0], x0, cmul(M.m[1], x1));
+                    y1 = cfma(M.m[2], x0, cmul(M.m[3], x1));
+                } else {
+                    y0 = cmul(M.m[1], x1);
+                    y1 = cmul(M.m[2], x0);
+                }
+            } else {
+                const int pm = 1 << r;
+                const float2 p0 = make_float2(__shfl_xor_sync(0xffffffffu, a[u].x, pm),
+                                              __shfl_xor_sync(0xffffffffu, a[u].y, pm));
+                const float2 p1 = make_float2(__shfl_xor_sync(0xffffffffu, a[u].z, pm),
+                                              __shfl_xor_sync(0xffffffffu, a[u].w, pm));
+                if (KIND == QS_K_DENSE) {
+                    y0 = one ? cfma(M.m[2], p0, cmul(M.m[3], x0)) : cfma(M.m[0], x0, cmul(M.m[1], p0));
+                    y1 = one ? cfma(M.m[2], p1, cmul(M.m[3], x1)) : cfma(M.m[0], x1, cmul(M.m[1], p1));
+                } else {
+                    y0 = one ? cmul(M.m[2], p0) : cmul(M.m[1], p0);
+                    y1 = one ? cmul(M.m[2], p1) : cmul(M.m[1], p1);
+                }
+            }
+            v4[q[u]] = make_float4(y0.x, y0.y, y1.x, y1.y);
+        }
+    }
+}
+
 // ------------------------------------------------------------- diagonal, flat
 // Walks the compact space of the non-fixed bits; amplitude i gets factor
 // D[sel(i)], sel built from up to two diagonal bits (hi, lo).  `fixed` bits are
@@ -465,6 +572,48 @@ int apply_1q_t(void* vec, int n, int bit, uint64_t cmask, int kind, const double
         launch_diag<V>(v, items, p, fixed, -1, bit, D, st);
         QS_CHECK_LAUNCH("qs_apply_1q(diag)");
         return QS_OK;
+    }
+    if (bit < 5 && (cmask & 31) != 0) {  // controls among the low bits: lanes on the free bits
+        // the 5 lowest non-control bits from `from` up, as a mask (0 if too few)
+        auto lane_bits = [&](int from) -> uint64_t {
+            uint64_t lm = 0;
+            int cnt = 0;
+            for (int b = from; b < n && cnt < 5; ++b)
+                if (!((cmask >> b) & 1)) {
+                    lm |= uint64_t(1) << b;
+                    ++cnt;
+                }
+            return cnt == 5 ? lm : 0;
+        };
+        if constexpr (sizeof(V) == 8) {
+            const uint64_t lm = (cmask & 1) ? 0 : lane_bits(1);
+            if (lm != 0) {
+                const int r = bit == 0 ? 0 : __builtin_popcountll(lm & ((uint64_t(1) << bit) - 1));
+                Plan p = make_plan(cmask | lm | 1);
+                const uint64_t chunks = uint64_t(1) << (n - p.nb);
+                const unsigned grid = grid_for(chunks, (kThreads / 32) * kUnroll, 8);
+                if (kind == QS_K_DENSE)
+                    k_1q_lanes_v2<QS_K_DENSE><<<grid, kThreads, 0, st>>>((float2*)v, chunks, p, cmask, lm, bit, r, M);
+                else
+                    k_1q_lanes_v2<QS_K_ANTIDIAG><<<grid, kThreads, 0, st>>>((float2*)v, chunks, p, cmask, lm, bit, r,
+                                                                           M);
+                QS_CHECK_LAUNCH("qs_apply_1q(low controls, float4)");
+                return QS_OK;
+            }
+        }
+        const uint64_t lm = lane_bits(0);
+        if (lm != 0) {
+            const int r = __builtin_popcountll(lm & ((uint64_t(1) << bit) - 1));
+            Plan p = make_plan(cmask | lm);
+            const uint64_t chunks = uint64_t(1) << (n - p.nb);
+            const unsigned grid = grid_for(chunks, (kThreads / 32) * kUnroll, 8);
+            if (kind == QS_K_DENSE)
+                k_1q_lanes<V, QS_K_DENSE><<<grid, kThreads, 0, st>>>(v, chunks, p, cmask, lm, r, M);
+            else
+                k_1q_lanes<V, QS_K_ANTIDIAG><<<grid, kThreads, 0, st>>>(v, chunks, p, cmask, lm, r, M);
+            QS_CHECK_LAUNCH("qs_apply_1q(low controls)");
+            return QS_OK;
+        }
     }
     if constexpr (sizeof(V) == 8) {
         if (bit < 5 && n >= 6) {  // 64-amplitude chunks, float4 per lane
