@@ -101,6 +101,35 @@ def test_persistent_hea_problems_and_graph_replays_are_identical(cuda_ok):
 
 
 @pytest.mark.gpu
+def test_persistent_linked_c128_every_stage_generated(cuda_ok):
+    """complex128 with EVERY register stage generated and linked into the
+    kernel (jit_min_qubits below every problem), QAOA and ansatz problems
+    together: the linked kernel runs, and matches per-instance complex128
+    runs to 1e-10."""
+    import torch
+    from quict_b200.differentiation import BatchedAdjoint, maxcut_observable, qaoa_circuit
+    from quict_b200.differentiation.persistent import PersistentBatch
+    from quict_b200.workloads import config3_problem
+    inst = _qaoa((10, 12, 14), seed=91)
+    probs = [(BatchedAdjoint(qaoa_circuit(n, e, p), maxcut_observable(n, e), "double"), prm) for n, e, p, prm in inst]
+    want = _reference(inst)
+    circ, obs, params = config3_problem(11, 2, 1)
+    e, g = BatchedAdjoint(circ, obs, "double").gradient(params[:1])
+    want.append((float(e[0]), g[0].cpu().numpy()))
+    probs.append((BatchedAdjoint(circ, obs, "double"), params[0]))
+    pb = PersistentBatch(probs, "double", caps=(11, 11), jit_min_qubits=9)
+    assert pb.sizes.jit_fns > 0
+    pb.capture()
+    pb.replay()
+    torch.cuda.synchronize()
+    res = pb.results()
+    assert pb.linked
+    for (e, g), (e2, g2) in zip(res, want):
+        assert abs(e - e2) < 1e-9
+        np.testing.assert_allclose(g, g2, rtol=0, atol=1e-9)
+
+
+@pytest.mark.gpu
 def test_persistent_wait_that_cannot_finish_times_out(cuda_ok):
     """Patch the plan so that the last work item waits for more items than
     its problem has: the bounded wait gives up after the timeout, control
