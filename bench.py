@@ -1,7 +1,7 @@
 """Benchmark: state-vector gate application at 30 qubits on B200.
 
 Workload (one step): StateVectorSimulator.run of the seeded 1000-gate
-config-1 circuit (gate set {H, X, Rx, Ry, Rz, U3, CX, CZ, Rzz, Swap} + 10% Haar
+spread circuit (gate set {H, X, Rx, Ry, Rz, U3, CX, CZ, Rzz, Swap} + 10% Haar
 2-qubit unitaries, qubits spread over vector bits < 5 and >= 20) on a
 30-qubit complex128 state (16 GiB): |0...0> initialisation + every gate.
 
@@ -17,8 +17,9 @@ roofline  the fused-pass kernel (qs_pass: each pass compiled at run time; the
         generic k_fused_reg runs a pass until its kernel is ready), bound fp64: algorithmic flops of
         its ops over its CUDA-event time, against cuBLAS DGEMM measured here;
         roofline_hbm: 2 * 2^n * 16 bytes per launch against MEASURED_PEAKS.json.
-single_gate_sweep, c64, configs_0_2, adjoint, qaoa  extra sections: per-gate HBM
-        fractions, complex64 at 30/32 qubits, configs 0 and 2, gradients, QAOA batch.
+single_gate_sweep, c64, public_api_runs, adjoint, qaoa  extra sections: per-gate HBM
+        fractions, complex64 at 30/32 qubits, the 20-qubit state-vector and 12-qubit
+        noisy density-matrix runs, ansatz gradients, the QAOA batch.
 cpu_baseline  the numba port of the reference CPU kernels (oracle/ref_port.py)
         on this host's cores: gates of every class of the same circuit timed,
         rate = 1000 / sum over classes (count x mean s/gate);
@@ -57,7 +58,7 @@ def ncu_traffic(n):
     """dram bytes per fused-pass launch from the committed ncu summary of the
     generated pass kernel (a 26-qubit capture scaled by the amplitudes
     processed), or None."""
-    for name in ("qs_pass_config1_c128.txt", "k_fused_reg_config1_c128.txt"):
+    for name in ("qs_pass_spread_c128.txt", "k_fused_reg_spread_c128.txt"):
         p = os.path.join(ROOT, "profiles", name)
         if os.path.exists(p):
             m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", open(p).read())
@@ -217,7 +218,7 @@ class CpuBaseline:
 
     def describe(self, gates_timed, seconds):
         counts = {c: len(i) for c, i in self.classes.items()}
-        return (f"{gates_timed} gates of the 1000-gate {self.n}q c128 config-1 circuit timed in {seconds:.1f} s, "
+        return (f"{gates_timed} gates of the 1000-gate {self.n}q c128 spread circuit timed in {seconds:.1f} s, "
                 f"stratified by gate class {counts}; rate = 1000 / sum(count x mean s/gate) "
                 f"(numba restatement of QuICT cpu_calculator kernels)")
 
@@ -248,8 +249,8 @@ def run_reference(args, ws, rank):
     thread) on the same workload; each step times one gate of every class."""
     if rank != 0:
         return
-    from quict_b200.workloads import config1_circuit
-    circuit = config1_circuit(N_QUBITS, N_GATES, SEED)
+    from quict_b200.workloads import spread_circuit
+    circuit = spread_circuit(N_QUBITS, N_GATES, SEED)
     cb = CpuBaseline(circuit, N_QUBITS)
     for _ in range(args.warmup):
         cb.sample(rounds=1, record=False)
@@ -258,15 +259,15 @@ def run_reference(args, ws, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "gates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded config-1 circuit)",
-        "config": {"workload": f"sv-{N_QUBITS}q-c128-{N_GATES}g-config1", "qubits": N_QUBITS,
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded spread circuit)",
+        "config": {"workload": f"sv-{N_QUBITS}q-c128-{N_GATES}g-spread", "qubits": N_QUBITS,
                    "gates_per_step": len(cb.classes), "seed": SEED},
         "cpu_baseline": {"value": v, "unit": "gates/s", "cores": cb.threads(), "kind": "port",
                          "s_per_gate_by_class": per, "sample": cb.describe(timed, secs)},
         "e2e": {"value": v, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if args.ref_one_thread:
-        line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: config1_circuit(q, N_GATES, SEED),
+        line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: spread_circuit(q, N_GATES, SEED),
                                                            n=N_QUBITS)
     print(json.dumps(line), flush=True)
 
@@ -285,14 +286,14 @@ def _events_ms(fn, reps):
 
 
 def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
-    """Device-timed gates/s of the config-1 circuit at n qubits (extra precisions / sizes)."""
+    """Device-timed gates/s of the spread circuit at n qubits (extra precisions / sizes)."""
     import torch
     from quict_b200 import _native as N
     from quict_b200.simulation import StateVectorSimulator
     from quict_b200.simulation.fusion import Pass
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
-    circuit = config1_circuit(n, N_GATES, SEED)
+    from quict_b200.workloads import spread_circuit
+    circuit = spread_circuit(n, N_GATES, SEED)
     sim = StateVectorSimulator("GPU", precision, gpu_device_id=local, sync=False, merge_bits=merge_bits)
     eng = sim.engine
     ops = lower_circuit(circuit.gates, n)
@@ -324,25 +325,25 @@ def sv_rate(n, precision, local, ws, steps=2, warmup=1, merge_bits=None):
     knobs = eng.knobs(vec, n).to_json()
     del sim, vec
     torch.cuda.empty_cache()
-    return {"workload": f"sv-{n}q-{'c128' if precision == 'double' else 'c64'}-{N_GATES}g-config1",
+    return {"workload": f"sv-{n}q-{'c128' if precision == 'double' else 'c64'}-{N_GATES}g-spread",
             "gates_per_s": ws * len(ops) / (ms / 1e3), "ms_per_run": ms, "fused_passes": passes,
             "knobs": knobs,
             "state_bytes": (1 << n) * (16 if precision == "double" else 8)}
 
 
 def c64_error(n, local):
-    """complex64 against complex128 on the config-1 circuit at n qubits (both
+    """complex64 against complex128 on the spread circuit at n qubits (both
     run by this GPU; the complex128 path is checked against the FP64 oracle
     and the per-gate kernels by the parity tests): max |amplitude error| and
     max error of <Z> on a spread of qubits (FP64 P(0) reductions)."""
     import numpy as np
     import torch
     from quict_b200.simulation import StateVectorSimulator
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     a = StateVectorSimulator("GPU", "double", gpu_device_id=local)
-    va = a.run(config1_circuit(n, N_GATES, SEED)).tensor
+    va = a.run(spread_circuit(n, N_GATES, SEED)).tensor
     b = StateVectorSimulator("GPU", "single", gpu_device_id=local)
-    vb = b.run(config1_circuit(n, N_GATES, SEED)).tensor
+    vb = b.run(spread_circuit(n, N_GATES, SEED)).tensor
     amp = 0.0
     for i in range(0, va.numel(), 1 << 27):
         amp = max(amp, float((va[i:i + (1 << 27)] - vb[i:i + (1 << 27)].to(torch.complex128)).abs().max()))
@@ -357,13 +358,13 @@ def c64_error(n, local):
 
 
 def grad_bench(ws, rank, local, batch=1024):
-    """Config 3: HEA 16q x 8 layers, 256 params, batch 1024 (split over ranks),
+    """Hardware-efficient-ansatz gradients: 16q x 8 layers, 256 params, batch 1024 (split over ranks),
     H = sum ZZ + 0.5 sum X.  Adjoint gradient (c64, c128) vs the same GPU's
     parameter shift (2 parameters timed, scaled to 256)."""
     import torch
     from quict_b200.differentiation import BatchedAdjoint
-    from quict_b200.workloads import config3_problem
-    circ, obs, params = config3_problem(16, 8, batch)
+    from quict_b200.workloads import hea_problem
+    circ, obs, params = hea_problem(16, 8, batch)
     from quict_b200.distributed import block_shard
     rows = block_shard(batch, ws, rank)
     per = len(rows)
@@ -397,7 +398,7 @@ def grad_bench(ws, rank, local, batch=1024):
 
 
 def qaoa_bench(ws, rank, local, count=512, graph_too=False):
-    """Config 4: uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6),
+    """Uneven QAOA MaxCut batch (n in 10..24 even, p in 1..6),
     complex64, instances split over ranks by amplitude x depth cost.  Timed:
     ONE persistent launch per rank (qs_batch_launch: every instance's forward
     passes, lam = C psi, energy, adjoint sweep and sums as work items; the
@@ -440,15 +441,15 @@ def qaoa_bench(ws, rank, local, count=512, graph_too=False):
     return out
 
 
-def small_configs_bench(ws, local, reps=3):
+def small_runs_bench(ws, local, reps=3):
     """Configs 0 and 2 through the public API, wall time per call with the
     device synchronised on both sides (host planning and copies included):
-    config 0 = StateVectorSimulator.run of the 20-qubit 200-gate circuit, then
-    sample(8192); config 2 = DensityMatrixSimulator.run of the 12-qubit
+    StateVectorSimulator.run of the 20-qubit 200-gate uniform circuit, then
+    sample(8192); DensityMatrixSimulator.run of the 12-qubit
     150-gate circuit with composed damping + depolarizing noise per gate."""
     import torch
     from quict_b200.simulation import DensityMatrixSimulator, StateVectorSimulator
-    from quict_b200.workloads import config0_circuit, config2_problem
+    from quict_b200.workloads import uniform_circuit, noisy_dm_problem
     dev = torch.device("cuda", local)
 
     def wall(fn):
@@ -464,16 +465,16 @@ def small_configs_bench(ws, local, reps=3):
         torch.cuda.synchronize(dev)
         return max_over_ranks((time.perf_counter() - t0) / reps * 1e3, ws)
 
-    c0 = config0_circuit(20, 200, 0)
+    c0 = uniform_circuit(20, 200, 0)
     sv = StateVectorSimulator("GPU", "double", gpu_device_id=local)
     run_ms = wall(lambda: sv.run(c0))
     sample_ms = wall(lambda: sv.sample(8192, seed=7))
-    c2, nm = config2_problem(12, 150, 2)
+    c2, nm = noisy_dm_problem(12, 150, 2)
     dm = DensityMatrixSimulator("GPU", "double", accumulated_mode=True, gpu_device_id=local)
     dm_ms = wall(lambda: dm.run(c2, noise_model=nm))
-    return {"config0": {"workload": "sv-20q-c128-200g-config0 + 8192 shots", "run_ms": run_ms,
+    return {"sv_20q": {"workload": "sv-20q-c128-200g-uniform + 8192 shots", "run_ms": run_ms,
                         "sample_8192_ms": sample_ms, "gates_per_s": ws * 200 / (run_ms / 1e3)},
-            "config2": {"workload": "dm-12q-c128-150g-damping+depolarizing", "run_ms": dm_ms,
+            "dm_12q": {"workload": "dm-12q-c128-150g-damping+depolarizing", "run_ms": dm_ms,
                         "gates_per_s": ws * 150 / (dm_ms / 1e3)},
             "timing": "wall clock per public call, device synchronised, max over ranks"}
 
@@ -587,7 +588,7 @@ def _sweep_pairs(n):
 
 
 def gate_sweep(eng, vec, n, ws, reps=5, warmup=2):
-    """Single-gate sweep: each gate class of the config-1 gate set applied by
+    """Single-gate sweep: each gate class of the spread-circuit gate set applied by
     its per-gate kernel to the resident n-qubit state at vector bits from the
     in-warp ones to the highest (``_sweep_bits`` / ``_sweep_pairs``);
     device-timed per launch; GB/s from ``sweep_bytes`` against the measured
@@ -625,10 +626,10 @@ def run_ours(args, ws, rank, local):
     from quict_b200 import _native as N
     from quict_b200.simulation import StateVectorSimulator
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
 
     n = args.qubits
-    circuit = config1_circuit(n, N_GATES, SEED)
+    circuit = spread_circuit(n, N_GATES, SEED)
     sim = StateVectorSimulator("GPU", "double", gpu_device_id=local, sync=False,
                                max_pass_cost=args.max_pass_cost, merge_bits=args.merge_bits,
                                tile_bits=args.tile_bits)
@@ -729,8 +730,8 @@ def run_ours(args, ws, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": "gates/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded config-1 circuit)",
-        "config": {"workload": f"sv-{n}q-c128-{N_GATES}g-config1", "qubits": n, "gates": len(ops),
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded spread circuit)",
+        "config": {"workload": f"sv-{n}q-c128-{N_GATES}g-spread", "qubits": n, "gates": len(ops),
                    "state_bytes": (1 << n) * 16, "fused_passes": npasses, "single_gate_launches": nsingle,
                    "knobs": eng.knobs(vec, n).to_json(), "knobs_source": knob_source(eng, vec, n),
                    "l2": f"inputs larger than L2 ({(1 << n) * 16 / 2**30:g} GiB state vs 126 MB L2)",
@@ -769,7 +770,7 @@ def run_ours(args, ws, rank, local):
             row.update(c64_error(nq, local))
             line["c64"].append(row)
     if not args.no_extra:
-        line["configs_0_2"] = small_configs_bench(ws, local)
+        line["public_api_runs"] = small_runs_bench(ws, local)
     if not args.no_grad:
         line["adjoint"] = grad_bench(ws, rank, local)
         line["qaoa"] = qaoa_bench(ws, rank, local, args.qaoa_instances, graph_too=args.qaoa_graph)
@@ -782,7 +783,7 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = {"value": r, "unit": "gates/s", "cores": cb.threads(), "kind": "port",
                                 "s_per_gate_by_class": per, "sample": cb.describe(timed, secs)}
         if args.ref_one_thread:
-            line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: config1_circuit(q, N_GATES, SEED), n=n)
+            line["cpu_baseline_1thread"] = one_thread_baseline(lambda q: spread_circuit(q, N_GATES, SEED), n=n)
     if rank == 0:
         # short summaries first: a reader of the line's head sees them
         head = {k: line[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step")}
@@ -806,14 +807,14 @@ def main():
     ap.add_argument("--ref-one-thread", type=int, default=1,
                     help="also time the port on one thread (26 qubits, scaled to 30)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-grad", action="store_true", help="skip the gradient (config 3/4) sections")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient sections (ansatz batch, QAOA batch)")
     ap.add_argument("--tile-bits", type=int, default=None, help="fused tile width k (default: the tuning cache)")
     ap.add_argument("--merge-bits", type=int, default=None,
                     help="gate-merging block width (0 disables; default: the tuning cache)")
     ap.add_argument("--no-extra", action="store_true", help="skip the complex64 30q / 32q runs")
     ap.add_argument("--qaoa-instances", type=int, default=512)
     ap.add_argument("--qaoa-graph", action="store_true",
-                    help="also time config 4 as per-instance kernel chains in one CUDA graph")
+                    help="also time the QAOA batch as per-instance kernel chains in one CUDA graph")
     ap.add_argument("--max-pass-cost", type=float, default=None,
                     help="fusion width: per-pass arithmetic bound in dense-1q-gate units (default: the tuning cache)")
     ap.add_argument("--jit", type=int, default=1,

@@ -538,7 +538,7 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
     // One tile buffer instead of two (kernels only): the next tile is fetched
     // after this one's stores, and the smaller footprint lets more CTAs share
     // an SM, whose loads and arithmetic overlap.  Measured on the 30-qubit
-    // config-1 circuit (B200): complex128 k = 10 316.7 -> 297.5 ms (8 instead of
+    // spread circuit (B200): complex128 k = 10 316.7 -> 297.5 ms (8 instead of
     // 6 CTAs per SM), complex64 k = 11 213.6 -> 226.8 ms; so the default is
     // single for complex128 and double for complex64.  QS_JIT_SINGLE_BUFFER=0/1
     // overrides it.

@@ -244,7 +244,7 @@ def main() -> None:
     """Tune the seeded random-circuit workloads and write the results to a cache file."""
     import torch
 
-    from ..workloads import config1_circuit
+    from ..workloads import spread_circuit
     from .engine import Engine
     from .lowering import lower_circuit
 
@@ -271,7 +271,7 @@ def main() -> None:
             dt = torch.complex128 if prec == "double" else torch.complex64
             vec = torch.empty(1 << n, dtype=dt, device=dev)
             eng = Engine(dev)
-            ops = lower_circuit(config1_circuit(n, a.gates, 1).gates, n)
+            ops = lower_circuit(spread_circuit(n, a.gates, 1).gates, n)
             res = tuner.tune(eng, vec, n, ops)
             print(json.dumps({"n": n, "precision": prec, "knobs": res.knobs.to_json(), "ms": res.ms}), flush=True)
             del vec

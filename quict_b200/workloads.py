@@ -1,11 +1,12 @@
-"""Seeded synthetic circuits with the shapes of the benchmark configurations.
+"""Seeded synthetic workloads.
 
-config0: n qubits, gates uniform over {H, X, Rx, Ry, Rz, U3, CX, CZ, Rzz,
-         Swap}, angles uniform in [0, 2 pi), distinct uniform qubits.
-config1: the same gate set plus 10% random Haar 2-qubit unitaries; every
-         qubit argument is drawn, with probability 1/2 each, from the qubits on
-         vector bits < 5 or from those on vector bits >= n - 10 (targets spread
-         over low and high bits).
+uniform circuit: n qubits, gates uniform over {H, X, Rx, Ry, Rz, U3, CX, CZ,
+         Rzz, Swap}, angles uniform in [0, 2 pi), distinct uniform qubits.
+spread circuit: the same gate set plus 10% random Haar 2-qubit unitaries;
+         every qubit argument is drawn, with probability 1/2 each, from the
+         qubits on vector bits < 5 or from those on vector bits >= n - 10
+         (targets spread over low and high bits).
+noisy density matrix, hardware-efficient ansatz: see their functions.
 All generators use numpy.random.default_rng(seed); nothing is read from disk.
 """
 from __future__ import annotations
@@ -14,7 +15,7 @@ import numpy as np
 
 from .core import GATE_BY_NAME, Circuit, Unitary
 
-CFG_GATES = ["h", "x", "rx", "ry", "rz", "u3", "cx", "cz", "rzz", "swap"]
+GATE_SET = ["h", "x", "rx", "ry", "rz", "u3", "cx", "cz", "rzz", "swap"]
 
 
 def haar_unitary(rng: np.random.Generator, d: int) -> np.ndarray:
@@ -24,13 +25,13 @@ def haar_unitary(rng: np.random.Generator, d: int) -> np.ndarray:
     return q * (np.diag(r) / np.abs(np.diag(r)))
 
 
-def config0_circuit(n: int = 20, size: int = 200, seed: int = 0) -> Circuit:
+def uniform_circuit(n: int = 20, size: int = 200, seed: int = 0) -> Circuit:
     c = Circuit(n)
     c.random_append(size, seed=seed)
     return c
 
 
-def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: float = 0.1) -> Circuit:
+def spread_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: float = 0.1) -> Circuit:
     rng = np.random.default_rng(seed)
     c = Circuit(n)
     low = [n - 1 - b for b in range(min(5, n))]                 # qubits on vector bits 0..4
@@ -49,7 +50,7 @@ def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: flo
         if rng.random() < haar_frac:
             Unitary(haar_unitary(rng, 4)) | c(pick(2))
             continue
-        nm = CFG_GATES[rng.integers(len(CFG_GATES))]
+        nm = GATE_SET[rng.integers(len(GATE_SET))]
         g = GATE_BY_NAME[nm]
         if g.params:
             g = g(*[float(x) for x in rng.uniform(0, 2 * np.pi, g.params)])
@@ -57,14 +58,14 @@ def config1_circuit(n: int = 30, size: int = 1000, seed: int = 1, haar_frac: flo
     return c
 
 
-def config2_problem(n: int = 12, size: int = 150, seed: int = 2, gamma: float = 5e-3, p1: float = 1e-3,
+def noisy_dm_problem(n: int = 12, size: int = 150, seed: int = 2, gamma: float = 5e-3, p1: float = 1e-3,
                     p2: float = 1e-2):
-    """Noisy density-matrix run: a `size`-gate circuit from the config-0 gate set,
+    """Noisy density-matrix run: a `size`-gate circuit from the uniform-circuit gate set,
     each gate followed by amplitude damping (gamma) composed with depolarizing
     noise (p1 for 1-qubit gates, p2 for 2-qubit gates) on the touched qubits.
     Returns (circuit, noise_model)."""
     from .core import DampingError, DepolarizingError, NoiseModel
-    c = config0_circuit(n, size, seed)
+    c = uniform_circuit(n, size, seed)
     one = ["h", "x", "rx", "ry", "rz", "u3"]
     two = ["cx", "cz", "rzz", "swap"]
     amp = DampingError(amplitude_prob=gamma, phase_prob=0)
@@ -74,7 +75,7 @@ def config2_problem(n: int = 12, size: int = 150, seed: int = 2, gamma: float = 
     return c, nm
 
 
-def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int = 3):
+def hea_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int = 3):
     """Hardware-efficient ansatz (Ry, Rz on every qubit + CZ ring per layer),
     H = sum Z_i Z_{i+1} (open chain) + 0.5 sum X_i, params uniform in [0, 2 pi)."""
     from .differentiation import hardware_efficient_ansatz, ising_observable
@@ -85,16 +86,16 @@ def config3_problem(n: int = 16, layers: int = 8, batch: int = 1024, seed: int =
 
 
 def sharded_run(qubits: int, precision: str, gates: int, seed: int = 1) -> dict:
-    """The config-1 style circuit on a vector sharded over every rank of the
+    """The spread circuit on a vector sharded over every rank of the
     default process group (one GPU per rank, NCCL), device-timed with CUDA
     events and reduced as the max over ranks."""
     import torch
     import torch.distributed as dist
 
     from .simulation.sharded import ShardedStateVector
-    circuit = config1_circuit(qubits, gates, seed)
+    circuit = spread_circuit(qubits, gates, seed)
     sv = ShardedStateVector(qubits, precision, device=torch.device("cuda", torch.cuda.current_device()))
-    sv.run(config1_circuit(qubits, 8, seed + 1))  # warm-up: knobs, matrix tables, communicators
+    sv.run(spread_circuit(qubits, 8, seed + 1))  # warm-up: knobs, matrix tables, communicators
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -106,7 +107,7 @@ def sharded_run(qubits: int, precision: str, gates: int, seed: int = 1) -> dict:
     t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    return {"workload": f"sv-{qubits}q-{precision}-{gates}g-config1 sharded over {sv.world} ranks",
+    return {"workload": f"sv-{qubits}q-{precision}-{gates}g-spread sharded over {sv.world} ranks",
             "ms": ms, "gates_per_s": gates / (ms / 1e3), "exchanges": sv.exchanges - ex0,
             "norm2": sv.norm2()}
 
@@ -171,7 +172,7 @@ def main() -> None:
               f"sum E = {sum(e for e, _ in res):.6e}")
         return
     from .differentiation import BatchedAdjoint
-    circ, obs, params = config3_problem(16, 8, a.batch)
+    circ, obs, params = hea_problem(16, 8, a.batch)
     eng = BatchedAdjoint(circ, obs, a.precision, tile_bits=a.tile_bits, pair_tile_bits=a.pair_tile_bits)
     gp = eng.plan_gradient(params)
     for _ in range(a.repeat):

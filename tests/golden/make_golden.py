@@ -14,7 +14,7 @@ Fixtures
   gates.json          matrix / matrix_type / arity of every reference gate type
   qasm_circuit.json   random_circuit_for_correction.qasm as a gate list
   qasm_state.npy      the reference's own golden state_vector.npy (10 qubits)
-  random_sv.npz       config-0 style random circuits (n=5, 8, 11), reference
+  random_sv.npz       uniform random circuits (n=5, 8, 11), reference
                       CPU StateVectorSimulator, double and single precision
   ext_sv.npz          every gate family incl. 3-qubit gates (n=6): reference
                       SV and reference UnitarySimulator
@@ -159,7 +159,7 @@ def core_fixtures(ref: str):
     json.dump({"n": n, "gates": gl}, open(os.path.join(HERE, "qasm_circuit.json"), "w"))
     np.save(os.path.join(HERE, "qasm_state.npy"), golden)
 
-    # ---- random config-0 circuits ---------------------------------------------------------
+    # ---- random uniform circuits ---------------------------------------------------------
     out = {}
     for n, size, seed in [(5, 40, 11), (8, 80, 12), (11, 120, 13)]:
         rng = np.random.default_rng(seed)

@@ -56,10 +56,10 @@ def test_autotuned_run_matches_oracle(cuda_ok, tmp_path, monkeypatch):
     from conftest import oracle_gates
     from oracle import sv as osv
     from quict_b200.simulation import StateVectorSimulator
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     monkeypatch.setenv("QUICT_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     n = 14
-    c = config1_circuit(n, 150, seed=3)
+    c = spread_circuit(n, 150, seed=3)
     sim = StateVectorSimulator("GPU", "double", autotune=True)
     v = sim.run(c).get()
     np.testing.assert_allclose(v, osv.run(oracle_gates(c), n), atol=1e-12)

@@ -59,9 +59,9 @@ def test_peak_source_and_plan_of_the_bench_circuit():
     assert peak > 1000 and kind in ("measured", "fallback")
     from quict_b200.simulation.fusion import Pass, plan
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     n = 30
-    ops = lower_circuit(config1_circuit(n, bench.N_GATES, bench.SEED).gates, n)
+    ops = lower_circuit(spread_circuit(n, bench.N_GATES, bench.SEED).gates, n)
     steps = plan(ops, n, 11, 5, merge_bits=2)
     passes = [s for s in steps if isinstance(s, Pass)]
     assert passes and all(bench.pass_flops(p, n) > 0 for p in passes)

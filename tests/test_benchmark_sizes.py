@@ -1,19 +1,20 @@
-"""Parity at the sizes the benchmark runs (configs 1-4 of bench.py).
+"""Parity at the sizes the benchmark runs (bench.py).
 
-* Config 1 (1000 gates, 10% Haar 2-qubit unitaries): at 30 qubits the fused
-  run against the per-gate kernels (independent code paths), complex64
+* The 1000-gate spread circuit (10% Haar 2-qubit unitaries): at 30 qubits the
+  fused run against the per-gate kernels (independent code paths), complex64
   against complex128, and the first 24 gates against the CPU port of the
   reference kernels on every amplitude; at 32 qubits (amplitude indices past
   2^31) complex64 against complex128 and fused against per-gate.  The fused
-  runs use the shipped tuning-cache knobs (c128 k = 11, c64 k = 12).
+  runs use the shipped tuning-cache knobs.
 * Every fused-pass knob the autotuner can pick, in both precisions, against
   the FP64 oracle.
-* Config 2 in full: 12-qubit density matrix, 150 noisy gates, against the
+* The noisy density matrix in full: 12 qubits, 150 noisy gates, against the
   FP64 superoperator oracle.
-* Config 3 in full: 16 qubits, 8 layers, 256 parameters, two parameter sets;
-  energies and adjoint gradients against the FP64 oracle's parameter shift.
-* Config 4 with instances up to 24 qubits: the batched complex64 graph
-  against per-instance complex128 runs.
+* The hardware-efficient-ansatz gradient in full: 16 qubits, 8 layers, 256
+  parameters, two parameter sets; energies and adjoint gradients against the
+  FP64 oracle's parameter shift.
+* The uneven QAOA batch with instances up to 24 qubits: the batched complex64
+  graph against per-instance complex128 runs.
 
 Tolerances: amplitudes 1e-12 (c128) / 1e-5 (c64); gradients 1e-10 (c128) /
 1e-4 (c64) of the FP64 oracle."""
@@ -61,21 +62,21 @@ def _sim(precision="double", **kw):
     return StateVectorSimulator("GPU", precision, **kw)
 
 
-def test_config1_30q_fused_vs_per_gate_and_c64_vs_c128(cuda_ok):
+def test_spread_30q_fused_vs_per_gate_and_c64_vs_c128(cuda_ok):
     import torch
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     n = 30
     if _free_gpu_bytes() < 40 * GiB:
         pytest.skip("needs 40 GiB of free device memory")
     a = _sim()
-    va = a.run(config1_circuit(n, 1000, 1)).tensor
+    va = a.run(spread_circuit(n, 1000, 1)).tensor
     b = _sim(fusion=False)
-    vb = b.run(config1_circuit(n, 1000, 1)).tensor
+    vb = b.run(spread_circuit(n, 1000, 1)).tensor
     assert _max_abs_diff(va, vb) < 1e-12
     del b, vb
     torch.cuda.empty_cache()
     s = _sim("single")
-    vs = s.run(config1_circuit(n, 1000, 1)).tensor
+    vs = s.run(spread_circuit(n, 1000, 1)).tensor
     assert _max_abs_diff(va, vs) < 1e-5
     bits = [0, 4, 15, 25, 29]
     dz = np.abs(_z_expectations(a, bits) - _z_expectations(s, bits))
@@ -83,18 +84,18 @@ def test_config1_30q_fused_vs_per_gate_and_c64_vs_c128(cuda_ok):
     assert abs(a.get_measured_prob(0, all_measured=True) - 1) < 1e-12
 
 
-def test_config1_30q_prefix_vs_cpu_port(cuda_ok):
+def test_spread_30q_prefix_vs_cpu_port(cuda_ok):
     """The first 24 gates at 30 qubits against the numba port of the reference
     CPU kernels (oracle/ref_port.py) on the host, on all 2^30 amplitudes."""
     import psutil
     from oracle import ref_port
     from quict_b200.core import Circuit
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     n = 30
     if psutil.virtual_memory().available < 48 * GiB:
         pytest.skip("needs 48 GiB of free host memory (two 16 GiB vectors)")
-    full = config1_circuit(n, 1000, 1)
+    full = spread_circuit(n, 1000, 1)
     pre = Circuit(n)
     pre.gates = full.gates[:24]
     v = _sim().run(pre).get()
@@ -106,25 +107,25 @@ def test_config1_30q_prefix_vs_cpu_port(cuda_ok):
     assert err < 1e-12
 
 
-def test_config1_32q_c64_vs_c128_and_fused_vs_per_gate(cuda_ok):
+def test_spread_32q_c64_vs_c128_and_fused_vs_per_gate(cuda_ok):
     """32 qubits: complex64 (32 GiB) against complex128 (64 GiB), and the
     complex128 fused run against the per-gate kernels (another 64 GiB)."""
     import torch
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     n = 32
     if _free_gpu_bytes() < 140 * GiB:
         pytest.skip("needs 140 GiB of free device memory")
     a = _sim()
-    va = a.run(config1_circuit(n, 1000, 1)).tensor
+    va = a.run(spread_circuit(n, 1000, 1)).tensor
     s = _sim("single")
-    vs = s.run(config1_circuit(n, 1000, 1)).tensor
+    vs = s.run(spread_circuit(n, 1000, 1)).tensor
     assert _max_abs_diff(va, vs) < 1e-5
     bits = [0, 4, 16, 27, 31]
     assert np.abs(_z_expectations(a, bits) - _z_expectations(s, bits)).max() < 1e-5
     del s, vs
     torch.cuda.empty_cache()
     b = _sim(fusion=False)
-    vb = b.run(config1_circuit(n, 1000, 1)).tensor
+    vb = b.run(spread_circuit(n, 1000, 1)).tensor
     assert _max_abs_diff(va, vb) < 1e-12
 
 
@@ -147,17 +148,17 @@ def test_every_tuner_candidate_vs_oracle(cuda_ok, precision):
             assert err < tol, (n, kn, err)
 
 
-def test_config2_full_12q_150_gates_vs_oracle(cuda_ok):
+def test_noisy_dm_12q_150_gates_vs_oracle(cuda_ok):
     """The benchmark's noisy density matrix in full: 12 qubits, 150 gates,
     each followed by damping composed with depolarizing noise."""
     from quict_b200.simulation import DensityMatrixSimulator
-    from quict_b200.workloads import config2_problem
-    c, nm = config2_problem(12, 150, 2)
+    from quict_b200.workloads import noisy_dm_problem
+    c, nm = noisy_dm_problem(12, 150, 2)
     k1, k2 = odm.composed_noise_1q(5e-3, 1e-3), odm.composed_noise_2q(5e-3, 1e-2)
     ref = odm.run(oracle_gates(c), 12, noise=lambda a: k1 if len(a) == 1 else k2, superop=True)
     rho = DensityMatrixSimulator("GPU", accumulated_mode=True).run(c, noise_model=nm).get()
     assert float(np.max(np.abs(rho - ref))) < 1e-12
-    c, nm = config2_problem(12, 150, 2)
+    c, nm = noisy_dm_problem(12, 150, 2)
     rho = DensityMatrixSimulator("GPU", "single", accumulated_mode=True).run(c, noise_model=nm).get()
     assert float(np.max(np.abs(rho - ref))) < 1e-5
 
@@ -197,13 +198,13 @@ def _param_shift_parallel(circ, params, terms):
     return g, oobs.energy(base, circ.n, terms)
 
 
-def test_config3_full_gradients_vs_fp64_parameter_shift(cuda_ok):
+def test_hea_16q_gradients_vs_fp64_parameter_shift(cuda_ok):
     """16 qubits, 8 layers of (Ry, Rz) + CZ ring, 256 parameters, H = sum ZZ +
     0.5 sum X: two parameter sets of the benchmark batch, adjoint gradients in
     both precisions against the FP64 oracle's parameter shift."""
     from quict_b200.differentiation import BatchedAdjoint
-    from quict_b200.workloads import config3_problem
-    circ, obs, params = config3_problem(16, 8, 1024)
+    from quict_b200.workloads import hea_problem
+    circ, obs, params = hea_problem(16, 8, 1024)
     rows = [0, 517]
     want = [_param_shift_parallel(circ, params[r], obs.terms) for r in rows]
     for precision, tol in (("double", 1e-10), ("single", 1e-4)):
@@ -214,7 +215,7 @@ def test_config3_full_gradients_vs_fp64_parameter_shift(cuda_ok):
             np.testing.assert_allclose(g[j].cpu().numpy(), gw, rtol=0, atol=tol)
 
 
-def test_config4_uneven_batch_up_to_24_qubits(cuda_ok):
+def test_uneven_qaoa_batch_up_to_24_qubits(cuda_ok):
     """The batched complex64 QAOA graph with instances of 10..24 qubits
     (two of 24) against per-instance complex128 adjoint runs."""
     import torch

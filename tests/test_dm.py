@@ -128,8 +128,8 @@ def test_dm_gpu_matches_reference_fixture(cuda_ok, n, fusion):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [7])
-def test_dm_config2_style_vs_oracle(cuda_ok, n):
-    """150-gate config-0 gate set with composed damping+depolarizing per gate,
+def test_dm_noisy_style_vs_oracle(cuda_ok, n):
+    """150-gate uniform-circuit gate set with composed damping+depolarizing per gate,
     against the Kraus-sum oracle (the 12-qubit run is checked in full against
     the superoperator oracle in test_benchmark_sizes.py)."""
     from quict_b200.core import Circuit

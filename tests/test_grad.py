@@ -157,7 +157,7 @@ def test_autograd_function(cuda_ok):
 
 @pytest.mark.gpu
 def test_uneven_qaoa_graph_vs_per_instance_c128(cuda_ok):
-    """Config-4 style batch (small sizes) in one CUDA graph, complex64, against
+    """Uneven QAOA batch (small sizes) in one CUDA graph, complex64, against
     per-instance complex128 adjoint runs and, for the smallest, the FP64 oracle."""
     from quict_b200.differentiation import (BatchedAdjoint, UnevenQAOABatch, qaoa_instances, qaoa_circuit,
                                             maxcut_observable)

@@ -1,6 +1,6 @@
 """Run-time compiled fused passes (qs_apply_fused_ex with the JIT on).
 
-CPU: the generator emits a source for every register launch of a config-1
+CPU: the generator emits a source for every register launch of a spread
 plan, and NVRTC compiles one for sm_100a.  GPU: with the JIT in SYNC mode
 (every register pass runs as its generated kernel) the results match the
 FP64 oracle and the generic kernels, for every tuner knob set and at the
@@ -20,10 +20,10 @@ def _plan_sources(n, esize, gates=300, knobs=None):
     from quict_b200.simulation.autotune import default_knobs
     from quict_b200.simulation.fusion import MatrixTable, Pass, emit, iter_plan, relabel_swaps
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     lib = N.load()
     kn = knobs or default_knobs(esize)
-    ops = relabel_swaps(lower_circuit(config1_circuit(n, gates, 1).gates, n), n)
+    ops = relabel_swaps(lower_circuit(spread_circuit(n, gates, 1).gates, n), n)
     passes = [s for s in iter_plan(ops, n, kn.tile_bits, kn.low_bits, merge_bits=kn.merge_bits)
               if isinstance(s, Pass) and s.ops]
     table = MatrixTable()
@@ -133,22 +133,22 @@ def test_compiled_passes_vs_oracle_for_every_tuner_knob(cuda_ok, jit_sync, preci
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["double", "single"])
 def test_compiled_passes_match_generic_kernels_at_26_qubits(cuda_ok, precision):
-    """The config-1 circuit at 26 qubits with the shipped knobs: compiled
+    """The spread circuit at 26 qubits with the shipped knobs: compiled
     passes against the generic register kernel."""
     import torch
     from quict_b200 import _native as N
     from quict_b200.simulation import StateVectorSimulator
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     tol = 1e-12 if precision == "double" else 1e-5
     prev = N.jit_set_mode(N.QS_JIT_OFF)
     try:
-        a = StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1)).tensor
+        a = StateVectorSimulator("GPU", precision).run(spread_circuit(26, 1000, 1)).tensor
         N.jit_set_mode(N.QS_JIT_ASYNC)  # queue every pass shape for the compile pool
-        StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1))
+        StateVectorSimulator("GPU", precision).run(spread_circuit(26, 1000, 1))
         N.jit_wait(900)
         N.jit_set_mode(N.QS_JIT_SYNC)
         before = N.jit_stats()["compiled_launches"]
-        b = StateVectorSimulator("GPU", precision).run(config1_circuit(26, 1000, 1)).tensor
+        b = StateVectorSimulator("GPU", precision).run(spread_circuit(26, 1000, 1)).tensor
         assert N.jit_stats()["compiled_launches"] >= before + 10
     finally:
         N.jit_set_mode(prev)
@@ -160,15 +160,15 @@ def test_compiled_passes_match_generic_kernels_at_26_qubits(cuda_ok, precision):
 def test_async_mode_switches_to_compiled_kernels(cuda_ok):
     from quict_b200 import _native as N
     from quict_b200.simulation import StateVectorSimulator
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     prev = N.jit_set_mode(N.QS_JIT_ASYNC)
     try:
-        c = config1_circuit(18, 200, 7)
+        c = spread_circuit(18, 200, 7)
         ref = osv.run(oracle_gates(c), 18)
-        v1 = StateVectorSimulator("GPU").run(config1_circuit(18, 200, 7)).get()
+        v1 = StateVectorSimulator("GPU").run(spread_circuit(18, 200, 7)).get()
         N.jit_wait(600)
         st = N.jit_stats()
-        v2 = StateVectorSimulator("GPU").run(config1_circuit(18, 200, 7)).get()
+        v2 = StateVectorSimulator("GPU").run(spread_circuit(18, 200, 7)).get()
         assert N.jit_stats()["compiled_launches"] > st["compiled_launches"]
         np.testing.assert_allclose(v1, ref, rtol=0, atol=1e-12)
         np.testing.assert_allclose(v2, ref, rtol=0, atol=1e-12)

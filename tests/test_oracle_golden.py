@@ -155,13 +155,13 @@ def test_cpu_port_reproduces_reference_states(n):
 
 
 def test_cpu_port_on_the_benchmark_circuit_shape():
-    """The port on a 12-qubit config-1 circuit (Haar 2q unitaries, low and high
+    """The port on a 12-qubit spread circuit (Haar 2q unitaries, low and high
     qubits) against the FP64 oracle, on all amplitudes."""
     from oracle import ref_port
     from quict_b200.simulation.lowering import lower_circuit
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
     n = 12
-    c = config1_circuit(n, 300, seed=3)
+    c = spread_circuit(n, 300, seed=3)
     v = osv.zero_state(n)
     ref_port.run(v, ref_port.prepare(lower_circuit(c.gates, n), np.complex128))
     np.testing.assert_allclose(v, osv.run(oracle_gates(c), n), rtol=0, atol=1e-12)

@@ -35,7 +35,7 @@ def _reference(inst):
 
 @pytest.mark.gpu
 def test_persistent_c64_matches_per_instance_c128_up_to_24_qubits(cuda_ok):
-    """Config-4 sizes (10..24 qubits, two of 24, depths 1..6) in one launch,
+    """Uneven-batch sizes (10..24 qubits, two of 24, depths 1..6) in one launch,
     complex64, against per-instance complex128 gradients."""
     import torch
     from quict_b200.differentiation import UnevenQAOABatch
@@ -78,10 +78,10 @@ def test_persistent_hea_problems_and_graph_replays_are_identical(cuda_ok):
     import torch
     from quict_b200.differentiation import BatchedAdjoint
     from quict_b200.differentiation.persistent import PersistentBatch
-    from quict_b200.workloads import config3_problem
+    from quict_b200.workloads import hea_problem
     probs, want = [], []
     for n, layers in ((10, 2), (12, 3), (14, 2)):
-        circ, obs, params = config3_problem(n, layers, 2)
+        circ, obs, params = hea_problem(n, layers, 2)
         ref = BatchedAdjoint(circ, obs, "double")
         e, g = ref.gradient(params[:1])
         want.append((float(e[0]), g[0].cpu().numpy()))
@@ -109,11 +109,11 @@ def test_persistent_linked_c128_every_stage_generated(cuda_ok):
     import torch
     from quict_b200.differentiation import BatchedAdjoint, maxcut_observable, qaoa_circuit
     from quict_b200.differentiation.persistent import PersistentBatch
-    from quict_b200.workloads import config3_problem
+    from quict_b200.workloads import hea_problem
     inst = _qaoa((10, 12, 14), seed=91)
     probs = [(BatchedAdjoint(qaoa_circuit(n, e, p), maxcut_observable(n, e), "double"), prm) for n, e, p, prm in inst]
     want = _reference(inst)
-    circ, obs, params = config3_problem(11, 2, 1)
+    circ, obs, params = hea_problem(11, 2, 1)
     e, g = BatchedAdjoint(circ, obs, "double").gradient(params[:1])
     want.append((float(e[0]), g[0].cpu().numpy()))
     probs.append((BatchedAdjoint(circ, obs, "double"), params[0]))

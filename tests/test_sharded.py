@@ -220,12 +220,12 @@ def test_solo_vector_on_the_gpu_engine(cuda_ok, precision, tol):
 
 def test_exchange_choice_looks_ahead():
     """Dry run of the placement (bit map only): a rank bit is traded for the
-    local bit whose next dense use is farthest away, so a config-1 style
+    local bit whose next dense use is farthest away, so a spread
     circuit (targets mostly in the low and high bits) needs about one
     exchange per rank bit instead of one per dense gate on a rank bit."""
     from quict_b200.simulation.lowering import lower_circuit
     from quict_b200.simulation.sharded import ShardedStateVector
-    from quict_b200.workloads import config1_circuit
+    from quict_b200.workloads import spread_circuit
 
     class Dry(ShardedStateVector):
         def __init__(self, n, world):
@@ -243,7 +243,7 @@ def test_exchange_choice_looks_ahead():
             pending.clear()
 
     n = 24
-    ops = lower_circuit(config1_circuit(n, 600, seed=3).gates, n)
+    ops = lower_circuit(spread_circuit(n, 600, seed=3).gates, n)
     for world in (2, 8):
         d = Dry(n, world)
         d.apply_ops(ops)

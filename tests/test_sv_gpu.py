@@ -44,7 +44,7 @@ def test_reference_golden_vector(cuda_ok, precision, fusion):
 
 @pytest.mark.parametrize("n", [5, 8, 11])
 @pytest.mark.parametrize("fusion", [True, False])
-def test_random_config0_circuits(cuda_ok, n, fusion):
+def test_random_uniform_circuits(cuda_ok, n, fusion):
     d = golden("random_sv.npz")
     gl = json.loads(str(d[f"n{n}_gates"]))
     v = sim("double", fusion=fusion).run(build_circuit(gl, n)).get()
@@ -111,7 +111,7 @@ def test_every_gate_every_placement_vs_oracle(cuda_ok, n, tile):
         np.testing.assert_allclose(v, ref, rtol=0, atol=1e-5)
 
 
-def test_config0_20q_200_gates(cuda_ok):
+def test_uniform_20q_200_gates(cuda_ok):
     from quict_b200.core import Circuit
     c = Circuit(20)
     c.random_append(200, seed=2024)
