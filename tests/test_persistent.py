@@ -263,3 +263,46 @@ def test_generated_stage_functions_compile_and_link_without_a_device():
     rc = N.load().qs_batch_link_check(C.byref(sz), C.byref(nb))
     assert rc == 0, N.load().qs_last_error()
     assert nb.value > 0
+
+
+def _items(blob):
+    """(kind, inst, need) of every work item in a written plan."""
+    nitems = int(blob[4:8].view(np.int32)[0])
+    off = int(blob[32:40].view(np.int64)[0])
+    rec = blob[off:off + 48 * nitems].reshape(nitems, 48)
+    kind = rec[:, 0:4].copy().view(np.int32)[:, 0]
+    inst = rec[:, 4:8].copy().view(np.int32)[:, 0]
+    need = rec[:, 16:24].copy().view(np.int64)[:, 0]
+    return kind, inst, need
+
+
+@pytest.mark.parametrize("group", ["0", "1", "2"])
+def test_planner_orders_every_wait_after_its_items(group, monkeypatch):
+    """The invariant the persistent kernel's deadlock freedom rests on, for
+    three problems and every interleaving: an item waits for exactly the items
+    of its problem's earlier stages, all of them come before it in the list,
+    no later item belongs to an earlier stage, and each problem's stages run
+    forward passes, lam = H psi, backward passes, final reduction in that
+    order."""
+    monkeypatch.setenv("QS_BATCH_GROUP", group)
+    inst, passes, ops, x, z, c, w = _tiny_plan_args()
+    three = (N.qs_batch_inst * 3)(inst[0], inst[0], inst[0])
+    rc, sz = _plan(three, passes, ops, x, z, c, w, tiles=1, amps=256)
+    assert rc == 0
+    blob = np.zeros(int(sz.blob_bytes), dtype=np.uint8)
+    rc, sz = _plan(three, passes, ops, x, z, c, w, tiles=1, amps=256, blob=blob.ctypes.data_as(C.c_void_p),
+                   nbytes=blob.nbytes)
+    assert rc == 0
+    kind, inst_of, need = _items(blob)
+    assert len(kind) == sz.nitems
+    for i in range(3):
+        seen = []  # (need, kind) of this problem's items so far, in list order
+        for k in np.nonzero(inst_of == i)[0]:
+            q = int(need[k])
+            assert q <= len(seen)                                   # what it waits for precedes it
+            assert sum(1 for p, _ in seen if p < q) == q            # exactly the earlier stages' items
+            assert all(p <= q for p, _ in seen)                     # stages never go backwards
+            seen.append((q, int(kind[k])))
+        stage_kinds = [kd for j, (q, kd) in enumerate(seen) if j == 0 or q != seen[j - 1][0]]
+        # forward (0), lam = H psi (1), backward (2), final (3)
+        assert stage_kinds == [0, 1, 2, 3]
