@@ -564,7 +564,12 @@ bool gen_reg_pass(const RegArgs& a, int R, const V* hm, JitPass& out, bool with_
         const char* e = getenv("QS_JIT_THREADS_PER_SM");
         return e && *e ? atoi(e) : 0;
     }();
-    const int target = env_target > 0 ? env_target : 512;
+    // 512 threads per SM; plain complex64 state-vector passes (no per-instance
+    // tables, no EXPECT ops) 256, i.e. the whole register file for 64-thread
+    // CTAs: on the 30-qubit spread circuit (B200, k = 11) 211.6 -> 189.7 ms
+    // (384: 208.2 ms).  complex128 passes are fastest at 512 (298 ms at 640,
+    // 344 ms at 768).
+    const int target = env_target > 0 ? env_target : (!C128 && !batched && a.nexp == 0 ? 256 : 512);
     const int minb = threads >= target ? 1 : target / threads;
     SrcBuf g;
     g.add("// generated fused pass: n=%d K=%d L=%d R=%d stages=%d ops=%d expect=%d batched=%d\n", a.n, K, L, R,
