@@ -91,6 +91,7 @@ struct Linked {
     void* mod[64] = {nullptr};
     void* fn[64] = {nullptr};
     int occ[64] = {0};
+    bool failed = false;  // a link or load failed once: callers run the generic kernel from then on
 };
 
 struct State {
@@ -429,8 +430,9 @@ std::string queue_device_fn(const std::string& src, const char* name) {
 // `keys` (empty on failure, with last_log set).  block: wait for the
 // functions' compilations; otherwise fail while any is pending.
 std::string link_cubin(const void* base, size_t base_size, const std::string& dispatcher,
-                       const std::vector<std::string>& keys, bool block) {
+                       const std::vector<std::string>& keys, bool block, bool* pending) {
     State& s = S();
+    if (pending) *pending = false;
     std::vector<std::shared_ptr<Entry>> es;
     {
         std::unique_lock<std::mutex> lock(s.mu);
@@ -451,6 +453,7 @@ std::string link_cubin(const void* base, size_t base_size, const std::string& di
         if (block) s.cv.wait(lock, all_done);
         if (!all_done()) {
             s.last_log = "link: device functions still compiling";
+            if (pending) *pending = true;
             return std::string();
         }
         for (const auto& e : es)
@@ -519,13 +522,18 @@ void* link_module(uint64_t link_key, const void* base, size_t base_size, const s
             *occ = it->second->occ[dev];
             return it->second->fn[dev];
         }
+        if (it != s.linked.end() && it->second->failed) return nullptr;
         if (!load || !load_driver(s)) return nullptr;
         if (it == s.linked.end()) it = s.linked.emplace(link_key, std::make_shared<Linked>()).first;
         lm = it->second;
     }
-    const std::string cubin = link_cubin(base, base_size, dispatcher, keys, block);
-    if (cubin.empty()) return nullptr;
+    bool pending = false;
+    const std::string cubin = link_cubin(base, base_size, dispatcher, keys, block, &pending);
     std::lock_guard<std::mutex> lock(s.mu);
+    if (cubin.empty()) {
+        if (!pending) lm->failed = true;  // still compiling: a later launch tries again; other failures are final
+        return nullptr;
+    }
     cudaFree(nullptr);  // the runtime's primary context is current from here on
     CUmodule mod = nullptr;
     CUresult r = s.api.module_load(&mod, cubin.data());
@@ -533,11 +541,13 @@ void* link_module(uint64_t link_key, const void* base, size_t base_size, const s
         const char* m = nullptr;
         s.api.cu_err(r, &m);
         s.last_log = std::string("cuModuleLoadData (linked batch kernel): ") + (m ? m : "error");
+        lm->failed = true;
         return nullptr;
     }
     CUfunction fn = nullptr;
     if (s.api.get_function(&fn, mod, kernel) != CUDA_SUCCESS) {
         s.last_log = std::string("cuModuleGetFunction failed for ") + kernel;
+        lm->failed = true;
         return nullptr;
     }
     int optin = 0;
@@ -547,6 +557,7 @@ void* link_module(uint64_t link_key, const void* base, size_t base_size, const s
     int nb = 0;
     if (s.api.occupancy(&nb, fn, threads, smem) != CUDA_SUCCESS || nb < 1) {
         s.last_log = "cuOccupancyMaxActiveBlocksPerMultiprocessor: the linked batch kernel does not fit an SM";
+        lm->failed = true;
         return nullptr;
     }
     lm->mod[dev] = mod;

@@ -36,9 +36,11 @@ std::string queue_device_fn(const std::string& src, const char* name);
 
 // The cubin link_module would load (no device needed): `base` linked with the
 // dispatcher (compiled here) and the compiled functions `keys`; empty on
-// failure (last_log says why).  block: wait for the functions' compilations.
+// failure (last_log says why; *pending, if given, is set when the failure is
+// only that some functions are still compiling).  block: wait for the
+// functions' compilations.
 std::string link_cubin(const void* base, size_t base_size, const std::string& dispatcher,
-                       const std::vector<std::string>& keys, bool block);
+                       const std::vector<std::string>& keys, bool block, bool* pending = nullptr);
 
 // Link the relocatable cubin `base` (the batch kernel), the `dispatcher`
 // source (compiled here) and the queued device functions `keys` with
@@ -46,7 +48,8 @@ std::string link_cubin(const void* base, size_t base_size, const std::string& di
 // kernel `kernel` (cached under link_key per device); *occ <- resident blocks
 // per SM at `threads` threads and `smem` dynamic shared memory.  block: wait
 // for the queued compilations; load == false (stream capture): only an
-// already linked kernel is returned.  Null on failure (last_log says why).
+// already linked kernel is returned.  Null on failure (last_log says why);
+// after a failure other than pending compilations it stays null for link_key.
 void* link_module(uint64_t link_key, const void* base, size_t base_size, const std::string& dispatcher,
                   const std::vector<std::string>& keys, const char* kernel, bool block, bool load, int threads,
                   size_t smem, int* occ);
